@@ -1,0 +1,718 @@
+// fl_capi.cu -- host runtime behind include/fiberlab_gpu.h: device tables,
+// per-slot workspaces, kernel dispatch over the built grid sizes, and the
+// C-ABI entry points.  Built for sm_100a only.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/fiberlab_gpu.h"
+#include "fl_launch.h"
+
+using namespace fl;
+
+struct fl_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    fl_ctx_opts opts{};
+    long launches = 0;
+    int sm_count = 0;
+};
+
+namespace {
+
+int set_err(fl_ctx* c, int code, const char* fmt, ...) {
+    if (c) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        c->err = buf;
+    }
+    return code;
+}
+
+#define CU(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? FL_ENOMEM : FL_ECUDA,  \
+                           "%s failed: %s", #call, cudaGetErrorString(e_));              \
+    } while (0)
+
+int ilog2i(int n) {
+    int l = 0;
+    while ((1 << l) < n) l++;
+    return l;
+}
+
+bool pow2(long n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// physics_models.jl:438-449
+bool hermitian(const double* hR, int nt) {
+    double mx = 1.0;
+    for (int k = 0; k < nt; k++) mx = std::max(mx, std::hypot(hR[2 * k], hR[2 * k + 1]));
+    const double tol = 1e-12 * mx;
+    if (std::fabs(hR[1]) > tol || std::fabs(hR[2 * (nt / 2) + 1]) > tol) return false;
+    for (int k = 1; k < nt / 2; k++) {
+        const int j = nt - k;
+        const double ar = hR[2 * k], ai = hR[2 * k + 1], br = hR[2 * j], bi = -hR[2 * j + 1];
+        const double d = std::hypot(ar - br, ai - bi);
+        const double m = std::max(std::hypot(ar, ai), std::hypot(br, bi));
+        if (d > std::max(tol, 1e-12 * m)) return false;
+    }
+    return true;
+}
+
+// sensitivity_disp_mmf.jl:103-112
+bool gamma_symmetric(const double* g, int m) {
+    double mx = 0.0;
+    const long m4 = (long)m * m * m * m;
+    for (long i = 0; i < m4; i++) mx = std::max(mx, std::fabs(g[i]));
+    const double tol = 1e-12 * std::max(1.0, mx);
+    auto at = [&](int i, int j, int k, int l) { return g[i + m * (j + m * (k + m * l))]; };
+    auto close = [&](double a, double b) {
+        return std::fabs(a - b) <= std::max(tol, 1e-12 * std::max(std::fabs(a), std::fabs(b)));
+    };
+    for (int l = 0; l < m; l++)
+        for (int k = 0; k < m; k++)
+            for (int j = 0; j < m; j++)
+                for (int i = 0; i < m; i++) {
+                    const double v = at(i, j, k, l);
+                    if (!close(v, at(j, i, k, l)) || !close(v, at(i, k, j, l)) ||
+                        !close(v, at(i, j, l, k)))
+                        return false;
+                }
+    return true;
+}
+
+__global__ void shaped_launch_kernel(const double2* __restrict__ u0,
+                                     const double* __restrict__ phases, int nt, int m,
+                                     int nbatch, double2* __restrict__ out, size_t out_stride) {
+    const long total = (long)nt * m * nbatch;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
+         i += (long)gridDim.x * blockDim.x) {
+        const int b = (int)(i / ((long)nt * m));
+        const long q = i % ((long)nt * m);
+        const int t = (int)(q % nt);
+        double s, c;
+        sincos(phases[(long)b * nt + t], &s, &c);
+        const double2 x = u0[q];
+        out[(size_t)b * out_stride + q] = make_double2(x.x * c - x.y * s, x.x * s + x.y * c);
+    }
+}
+
+__global__ void gather_stats_kernel(const SlotState* __restrict__ st, int n,
+                                    double* __restrict__ J) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) J[i] = st[i].J;
+}
+
+}  // namespace
+
+struct fl_problem {
+    fl_ctx* ctx = nullptr;
+    int nt = 0, m = 0, precision = 0;
+    double one_m_fR = 0, L = 0, reltol = 0, abstol = 0, gamma0 = 0;
+    bool gamma_sym = true;
+    double* d_Dturns = nullptr;
+    void* d_Heff = nullptr;
+    void* d_ss = nullptr;
+    void* d_tw = nullptr;
+    // workspace of the last forward (kept for fl_adjoint)
+    struct Work* last = nullptr;
+};
+
+// Per-batch workspace: one allocation carved into per-slot buffers.
+struct Work {
+    fl_ctx* ctx = nullptr;
+    int B = 0, nt = 0, rsize = 4, K = 0, segcap = 0, stepcap = 0, nsave = 0;
+    char* pool = nullptr;
+    size_t pool_bytes = 0;
+    void* d_desc = nullptr;          // SlotDesc<R>[B]
+    SlotState* d_state = nullptr;    // [B]
+    int* d_active = nullptr;         // [B]
+    std::vector<unsigned char> h_desc;  // host image of the descriptors
+    double* d_u0 = nullptr;          // per-slot launch (B * nt complex)
+    double* d_save = nullptr;        // per-slot save outputs (B * nsave * nt complex)
+    double* d_lamL = nullptr;        // per-slot seed (B * nt complex)
+    double* d_lam0 = nullptr;        // per-slot λ(0)
+    double* d_grad = nullptr;        // per-slot gradient (B * nt)
+    double* d_uL = nullptr;          // per-slot lab field at L
+    double* d_zsave = nullptr;
+    unsigned char* d_mask = nullptr;
+
+    ~Work() {
+        cudaFree(pool);
+        cudaFree(d_desc);
+        cudaFree(d_state);
+        cudaFree(d_active);
+    }
+};
+
+namespace {
+
+template <typename R>
+size_t slot_bytes(int nt, int K, int segcap, int stepcap) {
+    const size_t C = 2 * sizeof(R) * nt, D2 = 16 * (size_t)nt;
+    size_t b = 0;
+    b += 2 * D2 + 2 * D2;               // u[2], lam[2]
+    b += 14 * C;                        // kf, ka
+    b += 2 * C + C + sizeof(R) * nt;    // scr[2], esv, skv
+    b += (size_t)K * (D2 + C);          // checkpoints
+    b += 16 * (size_t)stepcap;          // step log
+    b += (size_t)segcap * 5 * C;        // recompute segment
+    return b + 64 * 32;                 // alignment slack
+}
+
+char* carve(char*& p, size_t bytes) {
+    char* r = p;
+    p += (bytes + 255) & ~size_t(255);
+    return r;
+}
+
+// Allocate a workspace for B slots; descriptors point into it.  Caller
+// buffers (u0 etc.) are per-slot arrays inside the workspace.
+template <typename R>
+int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
+    fl_ctx* ctx = pr->ctx;
+    auto w = std::make_unique<Work>();
+    w->ctx = ctx;
+    w->B = B;
+    w->nt = pr->nt;
+    w->rsize = sizeof(R);
+    w->K = ctx->opts.checkpoints;
+    w->segcap = ctx->opts.segment_steps;
+    w->stepcap = ctx->opts.step_log;
+    w->nsave = nsave;
+    const int nt = pr->nt;
+    const size_t per = slot_bytes<R>(nt, w->K, w->segcap, w->stepcap);
+    const size_t io = 16 * (size_t)nt * (2 + nsave + 2) + 8 * (size_t)nt + 256 * 8;
+    w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + nt + 4096;
+    if (ctx->opts.hbm_budget_bytes && w->pool_bytes > ctx->opts.hbm_budget_bytes)
+        return set_err(ctx, FL_OOM_ADMISSION, "workspace of %zu bytes exceeds the HBM budget",
+                       w->pool_bytes);
+    CU(cudaMalloc(&w->pool, w->pool_bytes));
+    CU(cudaMalloc(&w->d_desc, sizeof(SlotDesc<R>) * B));
+    CU(cudaMalloc(&w->d_state, sizeof(SlotState) * B));
+    CU(cudaMalloc(&w->d_active, sizeof(int) * B));
+    char* p = w->pool;
+    w->d_zsave = (double*)carve(p, 8 * (size_t)std::max(nsave, 1));
+    w->d_mask = (unsigned char*)carve(p, nt);
+    w->d_u0 = (double*)carve(p, 16 * (size_t)nt * B);
+    w->d_lamL = (double*)carve(p, 16 * (size_t)nt * B);
+    w->d_lam0 = (double*)carve(p, 16 * (size_t)nt * B);
+    w->d_uL = (double*)carve(p, 16 * (size_t)nt * B);
+    w->d_grad = (double*)carve(p, 8 * (size_t)nt * B);
+    w->d_save = nsave ? (double*)carve(p, 16 * (size_t)nt * nsave * B) : nullptr;
+    w->h_desc.resize(sizeof(SlotDesc<R>) * B);
+    SlotDesc<R>* hd = reinterpret_cast<SlotDesc<R>*>(w->h_desc.data());
+    const size_t C = 2 * sizeof(R) * nt, D2 = 16 * (size_t)nt;
+    for (int b = 0; b < B; b++) {
+        SlotDesc<R>& d = hd[b];
+        memset(&d, 0, sizeof d);
+        d.Dturns = pr->d_Dturns;
+        d.Heff = pr->d_Heff;
+        d.ss = pr->d_ss;
+        d.tw = pr->d_tw;
+        d.gamma = pr->gamma0;
+        d.one_m_fR = pr->one_m_fR;
+        d.L = pr->L;
+        d.reltol = pr->reltol;
+        d.abstol = pr->abstol;
+        d.mode = mode;
+        d.nsave = nsave;
+        d.ck_cap = w->K;
+        d.seg_cap = w->segcap;
+        d.step_cap = w->stepcap;
+        d.max_iters = ctx->opts.max_iters;
+        d.zsave = w->d_zsave;
+        d.save_out = nsave ? w->d_save + (size_t)b * 2 * nt * nsave : nullptr;
+        d.u0 = w->d_u0 + (size_t)b * 2 * nt;
+        d.mask = w->d_mask;
+        d.lamL = w->d_lamL + (size_t)b * 2 * nt;
+        d.lam0_out = w->d_lam0 + (size_t)b * 2 * nt;
+        d.grad_out = w->d_grad + (size_t)b * nt;
+        d.uL_out = w->d_uL + (size_t)b * 2 * nt;
+        d.u[0] = (double*)carve(p, D2);
+        d.u[1] = (double*)carve(p, D2);
+        d.lam[0] = (double*)carve(p, D2);
+        d.lam[1] = (double*)carve(p, D2);
+        for (int i = 0; i < 7; i++) d.kf[i] = carve(p, C);
+        for (int i = 0; i < 7; i++) d.ka[i] = carve(p, C);
+        d.scr[0] = carve(p, C);
+        d.scr[1] = carve(p, C);
+        d.esv = carve(p, C);
+        d.skv = carve(p, sizeof(R) * nt);
+        d.ck_u = (double*)carve(p, D2 * w->K);
+        d.ck_k1 = carve(p, C * w->K);
+        d.steplog = (double*)carve(p, 16 * (size_t)w->stepcap);
+        d.seg = carve(p, C * 5 * (size_t)w->segcap);
+    }
+    if ((size_t)(p - w->pool) > w->pool_bytes)
+        return set_err(ctx, FL_ECUDA, "internal: workspace overflow (%zu > %zu)",
+                       (size_t)(p - w->pool), w->pool_bytes);
+    CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), w->h_desc.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    std::vector<int> act(B);
+    for (int b = 0; b < B; b++) act[b] = b;
+    CU(cudaMemcpyAsync(w->d_active, act.data(), sizeof(int) * B, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState) * B, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    *out = w.release();
+    return FL_OK;
+}
+
+int launch_slots(fl_ctx* ctx, fl_problem* pr, Work* w, int nactive, int max_evals) {
+    const int logn = ilog2i(pr->nt);
+    const int fp64 = pr->precision == FL_PRECISION_FP64;
+    LaunchFn fn = sm_launcher(fp64, logn);
+    if (!fn)
+        return set_err(ctx, FL_EUNSUPPORTED, "Nt = 2^%d is not built for %s", logn,
+                       fp64 ? "FP64" : "FP32");
+    LaunchArgs a{w->d_desc, w->d_state, w->d_active, nactive, max_evals, ctx->stream};
+    CU(fn(a));
+    ctx->launches++;
+    return FL_OK;
+}
+
+int run_to_completion(fl_problem* pr, Work* w) {
+    fl_ctx* ctx = pr->ctx;
+    int rc = launch_slots(ctx, pr, w, w->B, 0x7fffffff);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
+int read_states(fl_ctx* ctx, Work* w, std::vector<SlotState>& st) {
+    st.resize(w->B);
+    CU(cudaMemcpyAsync(st.data(), w->d_state, sizeof(SlotState) * w->B, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
+void fill_stats(const SlotState& s, fl_stats* o) {
+    o->naccept = s.naccept;
+    o->nreject = s.nreject;
+    o->nf = s.nf;
+    o->adj_naccept = s.a_naccept;
+    o->adj_nreject = s.a_nreject;
+    o->adj_nf = s.a_nf;
+    o->status = s.status;
+    o->checkpoints_used = s.ck_stride > 0 ? (s.nsteps + s.ck_stride - 1) / s.ck_stride : 0;
+    o->J = s.J;
+    o->z_end = s.z;
+}
+
+int check_problem(fl_problem* pr) {
+    if (!pr || !pr->ctx) return FL_EINVAL;
+    if (pr->m != 1)
+        return set_err(pr->ctx, FL_EUNSUPPORTED,
+                       "multimode problems (M=%d) go through the multimode stepper", pr->m);
+    return FL_OK;
+}
+
+template <typename R>
+int upload_tables(fl_problem* pr, const double* D, const double* hR, const double* ss) {
+    fl_ctx* ctx = pr->ctx;
+    const int nt = pr->nt, m = pr->m;
+    std::vector<double> dturn((size_t)nt * m);
+    for (size_t i = 0; i < dturn.size(); i++) dturn[i] = D[i] / (2.0 * M_PI);
+    std::vector<R> heff(2 * (size_t)nt), ssv(nt), tw(2 * (size_t)nt);
+    for (int k = 0; k < nt; k++) {
+        const double sg = (k & 1) ? -1.0 : 1.0;  // fftshift folded into the response
+        heff[2 * k] = (R)(hR[2 * k] * sg);
+        heff[2 * k + 1] = (R)(hR[2 * k + 1] * sg);
+        ssv[k] = (R)ss[k];
+        const double a = -2.0 * M_PI * (double)k / (double)nt;
+        tw[2 * k] = (R)std::cos(a);
+        tw[2 * k + 1] = (R)std::sin(a);
+    }
+    CU(cudaMalloc(&pr->d_Dturns, sizeof(double) * dturn.size()));
+    CU(cudaMalloc(&pr->d_Heff, sizeof(R) * heff.size()));
+    CU(cudaMalloc(&pr->d_ss, sizeof(R) * ssv.size()));
+    CU(cudaMalloc(&pr->d_tw, sizeof(R) * tw.size()));
+    CU(cudaMemcpy(pr->d_Dturns, dturn.data(), sizeof(double) * dturn.size(),
+                  cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_Heff, heff.data(), sizeof(R) * heff.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_ss, ssv.data(), sizeof(R) * ssv.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_tw, tw.data(), sizeof(R) * tw.size(), cudaMemcpyHostToDevice));
+    return FL_OK;
+}
+
+int status_of_slots(fl_ctx* ctx, const std::vector<SlotState>& st) {
+    for (size_t i = 0; i < st.size(); i++)
+        if (st[i].status != ST_OK)
+            return set_err(ctx, st[i].status, "slot %zu: %s", i, fl_status_string(st[i].status));
+    return FL_OK;
+}
+
+int new_work(fl_problem* pr, int B, int nsave, int mode, Work** w) {
+    return pr->precision == FL_PRECISION_FP64 ? work_create<double>(pr, B, nsave, mode, w)
+                                              : work_create<float>(pr, B, nsave, mode, w);
+}
+
+// rewrite the mode of every descriptor (host image + device copy)
+int set_mode(fl_ctx* ctx, Work* w, int mode, int log_cost) {
+    const size_t dsz = w->rsize == 8 ? sizeof(SlotDesc<double>) : sizeof(SlotDesc<float>);
+    for (int b = 0; b < w->B; b++) {
+        unsigned char* base = w->h_desc.data() + (size_t)b * dsz;
+        if (w->rsize == 8) {
+            reinterpret_cast<SlotDesc<double>*>(base)->mode = mode;
+            reinterpret_cast<SlotDesc<double>*>(base)->log_cost = log_cost;
+        } else {
+            reinterpret_cast<SlotDesc<float>*>(base)->mode = mode;
+            reinterpret_cast<SlotDesc<float>*>(base)->log_cost = log_cost;
+        }
+    }
+    CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), w->h_desc.size(), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    return FL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* fl_version(void) { return "fiberlab-gpu 0.1 (sm_100a)"; }
+
+const char* fl_status_string(int s) {
+    switch (s) {
+        case FL_OK: return "ok";
+        case FL_EINVAL: return "invalid argument";
+        case FL_NONFINITE: return "non-finite value in the solution";
+        case FL_DT_UNDERFLOW: return "step size below floating-point resolution";
+        case FL_MAXITERS: return "maximum attempted steps reached";
+        case FL_ENOMEM: return "device out of memory";
+        case FL_NONSYMMETRIC: return "adjoint requires a permutation-symmetric gamma tensor";
+        case FL_ENODEV: return "no usable CUDA device";
+        case FL_ECUDA: return "CUDA runtime error";
+        case FL_ECAPACITY: return "checkpoint / segment / step-log capacity exceeded";
+        case FL_EUNSUPPORTED: return "unsupported shape";
+        case FL_OOM_ADMISSION: return "request exceeds the HBM budget";
+        case FL_EBUSY: return "request not finished";
+        case FL_TIMEOUT: return "wait limit reached";
+        default: return "unknown status";
+    }
+}
+
+int fl_ctx_create(int device, const fl_ctx_opts* opts, fl_ctx** out) {
+    if (!out) return FL_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) return FL_ENODEV;
+    fl_ctx* ctx = new (std::nothrow) fl_ctx();
+    if (!ctx) return FL_ENOMEM;
+    ctx->device = device;
+    ctx->opts.hbm_budget_bytes = 0;
+    ctx->opts.checkpoints = 32;
+    ctx->opts.segment_steps = 16;
+    ctx->opts.step_log = 16384;
+    ctx->opts.max_iters = 100000;
+    if (opts) {
+        if (opts->hbm_budget_bytes) ctx->opts.hbm_budget_bytes = opts->hbm_budget_bytes;
+        if (opts->checkpoints) ctx->opts.checkpoints = opts->checkpoints;
+        if (opts->segment_steps) ctx->opts.segment_steps = opts->segment_steps;
+        if (opts->step_log) ctx->opts.step_log = opts->step_log;
+        if (opts->max_iters) ctx->opts.max_iters = opts->max_iters;
+    }
+    if (!pow2(ctx->opts.checkpoints) || ctx->opts.checkpoints < 2 ||
+        ctx->opts.segment_steps < 1 || ctx->opts.step_log < 1 || ctx->opts.max_iters < 1) {
+        delete ctx;
+        return FL_EINVAL;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete ctx;
+        return FL_ENODEV;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        delete ctx;
+        return FL_ENODEV;
+    }
+    ctx->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return FL_ECUDA;
+    }
+    *out = ctx;
+    return FL_OK;
+}
+
+int fl_ctx_destroy(fl_ctx* ctx) {
+    if (!ctx) return FL_EINVAL;
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return FL_OK;
+}
+
+const char* fl_last_error(const fl_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+long fl_ctx_launch_count(const fl_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int fl_ctx_synchronize(fl_ctx* ctx) {
+    if (!ctx) return FL_EINVAL;
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
+int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double* gamma,
+                      const double* hR, const double* selfsteep, double one_m_fR, double L,
+                      double reltol, double abstol, int precision, fl_problem** out) {
+    if (!ctx || !out) return FL_EINVAL;
+    *out = nullptr;
+    if (nt < 4 || !pow2(nt)) return set_err(ctx, FL_EINVAL, "Nt must be a power of two >= 4");
+    if (m < 1) return set_err(ctx, FL_EINVAL, "M must be a positive integer");
+    if (!D || !gamma || !hR || !selfsteep) return set_err(ctx, FL_EINVAL, "null table");
+    if (precision != FL_PRECISION_FP32 && precision != FL_PRECISION_FP64)
+        return set_err(ctx, FL_EINVAL, "unknown precision %d", precision);
+    if (!(std::isfinite(L) && L > 0)) return set_err(ctx, FL_EINVAL, "L must be positive and finite");
+    if (!(std::isfinite(reltol) && reltol > 0))
+        return set_err(ctx, FL_EINVAL, "reltol must be positive and finite");
+    if (!(std::isfinite(abstol) && abstol > 0))
+        return set_err(ctx, FL_EINVAL, "abstol must be positive and finite");
+    if (!std::isfinite(one_m_fR)) return set_err(ctx, FL_EINVAL, "one_m_fR must be finite");
+    const long m4 = (long)m * m * m * m;
+    for (long i = 0; i < m4; i++)
+        if (!std::isfinite(gamma[i])) return set_err(ctx, FL_EINVAL, "gamma tensor must be finite");
+    for (long i = 0; i < (long)nt * m; i++)
+        if (!std::isfinite(D[i])) return set_err(ctx, FL_EINVAL, "dispersion must be finite");
+    for (int i = 0; i < 2 * nt; i++)
+        if (!std::isfinite(hR[i])) return set_err(ctx, FL_EINVAL, "Raman response must be finite");
+    for (int i = 0; i < nt; i++)
+        if (!std::isfinite(selfsteep[i])) return set_err(ctx, FL_EINVAL, "selfsteep must be finite");
+    if (!hermitian(hR, nt))
+        return set_err(ctx, FL_EINVAL, "Raman response spectrum must be Hermitian");
+    auto pr = std::make_unique<fl_problem>();
+    pr->ctx = ctx;
+    pr->nt = nt;
+    pr->m = m;
+    pr->precision = precision;
+    pr->one_m_fR = one_m_fR;
+    pr->L = L;
+    pr->reltol = reltol;
+    pr->abstol = abstol;
+    pr->gamma0 = gamma[0];
+    pr->gamma_sym = gamma_symmetric(gamma, m);
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    int rc = precision == FL_PRECISION_FP64 ? upload_tables<double>(pr.get(), D, hR, selfsteep)
+                                            : upload_tables<float>(pr.get(), D, hR, selfsteep);
+    if (rc) {
+        fl_problem_destroy(pr.release());
+        return rc;
+    }
+    *out = pr.release();
+    return FL_OK;
+}
+
+int fl_problem_destroy(fl_problem* pr) {
+    if (!pr) return FL_EINVAL;
+    delete pr->last;
+    cudaFree(pr->d_Dturns);
+    cudaFree(pr->d_Heff);
+    cudaFree(pr->d_ss);
+    cudaFree(pr->d_tw);
+    delete pr;
+    return FL_OK;
+}
+
+int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave,
+               double* out_spectra, fl_stats* stats) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!u0 || nsave < 0 || (nsave > 0 && (!saveat || !out_spectra)))
+        return set_err(ctx, FL_EINVAL, "null argument");
+    // propagation.jl:60-70: sorted, unique, starts at 0 and ends at L
+    if (nsave > 0) {
+        if (nsave < 2) return set_err(ctx, FL_EINVAL, "saveat must include 0 and the fiber length");
+        for (int i = 0; i < nsave; i++)
+            if (!std::isfinite(saveat[i])) return set_err(ctx, FL_EINVAL, "saveat distances must be finite");
+        for (int i = 1; i < nsave; i++)
+            if (!(saveat[i] > saveat[i - 1]))
+                return set_err(ctx, FL_EINVAL, "saveat distances must be sorted and unique");
+        if (saveat[0] != 0.0 || saveat[nsave - 1] != pr->L)
+            return set_err(ctx, FL_EINVAL, "saveat must start at 0 and end at the fiber length");
+    }
+    const int nt = pr->nt;
+    double nrm = 0.0;
+    for (int i = 0; i < 2 * nt * pr->m; i++) {
+        if (!std::isfinite(u0[i])) return set_err(ctx, FL_EINVAL, "input spectrum must be finite");
+        nrm += u0[i] * u0[i];
+    }
+    if (!(nrm > 0)) return set_err(ctx, FL_EINVAL, "input spectrum must be nonzero");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    delete pr->last;
+    pr->last = nullptr;
+    Work* w = nullptr;
+    rc = new_work(pr, 1, nsave, MODE_FORWARD, &w);
+    if (rc) return rc;
+    pr->last = w;
+    CU(cudaMemcpyAsync(w->d_u0, u0, 16 * (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
+    if (nsave)
+        CU(cudaMemcpyAsync(w->d_zsave, saveat, 8 * (size_t)nsave, cudaMemcpyHostToDevice,
+                           ctx->stream));
+    rc = run_to_completion(pr, w);
+    if (rc) return rc;
+    std::vector<SlotState> st;
+    rc = read_states(ctx, w, st);
+    if (rc) return rc;
+    if (stats) fill_stats(st[0], stats);
+    if (st[0].status) return set_err(ctx, st[0].status, "%s", fl_status_string(st[0].status));
+    if (nsave)
+        CU(cudaMemcpy(out_spectra, w->d_save, 16 * (size_t)nt * nsave, cudaMemcpyDeviceToHost));
+    return FL_OK;
+}
+
+int fl_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats* stats) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!lambdaL || !lambda0) return set_err(ctx, FL_EINVAL, "null argument");
+    if (!pr->gamma_sym)
+        return set_err(ctx, FL_NONSYMMETRIC,
+                       "fiber adjoint requires a fully permutation-symmetric gamma tensor");
+    if (!pr->last) return set_err(ctx, FL_EINVAL, "fl_adjoint needs a preceding fl_forward");
+    const int nt = pr->nt;
+    for (int i = 0; i < 2 * nt * pr->m; i++)
+        if (!std::isfinite(lambdaL[i]))
+            return set_err(ctx, FL_EINVAL, "adjoint terminal condition must be finite");
+    Work* w = pr->last;
+    std::vector<SlotState> st;
+    rc = read_states(ctx, w, st);
+    if (rc) return rc;
+    if (st[0].phase != PH_DONE || st[0].status != ST_OK)
+        return set_err(ctx, FL_EINVAL, "the last forward did not complete");
+    st[0].phase = PH_SEED;
+    CU(cudaMemcpyAsync(w->d_state, st.data(), sizeof(SlotState), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    rc = set_mode(ctx, w, MODE_SEEDED_ADJOINT, 0);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(w->d_lamL, lambdaL, 16 * (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
+    rc = run_to_completion(pr, w);
+    if (rc) return rc;
+    rc = read_states(ctx, w, st);
+    if (rc) return rc;
+    if (stats) fill_stats(st[0], stats);
+    if (st[0].status) return set_err(ctx, st[0].status, "%s", fl_status_string(st[0].status));
+    CU(cudaMemcpy(lambda0, w->d_lam0, 16 * (size_t)nt, cudaMemcpyDeviceToHost));
+    return FL_OK;
+}
+
+static int phase_gradient_core(fl_problem* pr, Work* w, int nbatch, const double* d_u0,
+                               const double* d_phases, const unsigned char* d_mask,
+                               int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+    fl_ctx* ctx = pr->ctx;
+    const int nt = pr->nt;
+    int rc = set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost);
+    if (rc) return rc;
+    CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState) * nbatch, ctx->stream));
+    CU(cudaMemcpyAsync(w->d_mask, d_mask, nt, cudaMemcpyDeviceToDevice, ctx->stream));
+    const int threads = 256;
+    const long total = (long)nt * nbatch;
+    const int blocks = (int)std::min<long>((total + threads - 1) / threads, 4096);
+    shaped_launch_kernel<<<blocks, threads, 0, ctx->stream>>>(
+        (const double2*)d_u0, d_phases, nt, 1, nbatch, (double2*)w->d_u0, (size_t)nt);
+    ctx->launches++;
+    CU(cudaGetLastError());
+    rc = run_to_completion(pr, w);
+    if (rc) return rc;
+    gather_stats_kernel<<<(nbatch + 255) / 256, 256, 0, ctx->stream>>>(w->d_state, nbatch, d_J);
+    ctx->launches++;
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(d_grad, w->d_grad, 8 * (size_t)nt * nbatch, cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    std::vector<SlotState> st;
+    rc = read_states(ctx, w, st);
+    if (rc) return rc;
+    if (stats)
+        for (int b = 0; b < nbatch; b++) fill_stats(st[b], &stats[b]);
+    return status_of_slots(ctx, st);
+}
+
+int fl_phase_gradient_batch_device(fl_problem* pr, const double* d_u0, int nbatch,
+                                   const double* d_phases, const unsigned char* d_mask,
+                                   int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!d_u0 || !d_phases || !d_mask || !d_J || !d_grad || nbatch < 1)
+        return set_err(ctx, FL_EINVAL, "null argument");
+    if (!pr->gamma_sym)
+        return set_err(ctx, FL_NONSYMMETRIC,
+                       "fiber adjoint requires a fully permutation-symmetric gamma tensor");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    // keep one workspace per problem sized for the largest batch seen
+    if (!pr->last || pr->last->B < nbatch || pr->last->nsave != 0) {
+        delete pr->last;
+        pr->last = nullptr;
+        Work* w = nullptr;
+        rc = new_work(pr, nbatch, 0, MODE_BAND_GRADIENT, &w);
+        if (rc) return rc;
+        pr->last = w;
+    }
+    Work* w = pr->last;
+    const int B = w->B;
+    if (B != nbatch) {
+        // run only the first nbatch slots
+        w->B = nbatch;
+        rc = phase_gradient_core(pr, w, nbatch, d_u0, d_phases, d_mask, log_cost, d_J, d_grad,
+                                 stats);
+        w->B = B;
+        return rc;
+    }
+    return phase_gradient_core(pr, w, nbatch, d_u0, d_phases, d_mask, log_cost, d_J, d_grad,
+                               stats);
+}
+
+int fl_phase_gradient_batch(fl_problem* pr, const double* u0, int nbatch, const double* phases,
+                            const unsigned char* mask, int log_cost, double* J, double* grad,
+                            fl_stats* stats) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!u0 || !phases || !mask || !J || !grad || nbatch < 1)
+        return set_err(ctx, FL_EINVAL, "null argument");
+    const int nt = pr->nt;
+    bool any = false;
+    for (int i = 0; i < nt; i++) any |= mask[i] != 0;
+    if (!any) return set_err(ctx, FL_EINVAL, "band mask must contain at least one bin");
+    for (long i = 0; i < (long)nt * nbatch; i++)
+        if (!std::isfinite(phases[i])) return set_err(ctx, FL_EINVAL, "phase values must be finite");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    double *d_u0 = nullptr, *d_ph = nullptr, *d_J = nullptr, *d_g = nullptr;
+    unsigned char* d_m = nullptr;
+    CU(cudaMallocAsync(&d_u0, 16 * (size_t)nt, ctx->stream));
+    CU(cudaMallocAsync(&d_ph, 8 * (size_t)nt * nbatch, ctx->stream));
+    CU(cudaMallocAsync(&d_J, 8 * (size_t)nbatch, ctx->stream));
+    CU(cudaMallocAsync(&d_g, 8 * (size_t)nt * nbatch, ctx->stream));
+    CU(cudaMallocAsync(&d_m, nt, ctx->stream));
+    CU(cudaMemcpyAsync(d_u0, u0, 16 * (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(d_ph, phases, 8 * (size_t)nt * nbatch, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(d_m, mask, nt, cudaMemcpyHostToDevice, ctx->stream));
+    rc = fl_phase_gradient_batch_device(pr, d_u0, nbatch, d_ph, d_m, log_cost, d_J, d_g, stats);
+    if (rc == FL_OK) {
+        CU(cudaMemcpyAsync(J, d_J, 8 * (size_t)nbatch, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(grad, d_g, 8 * (size_t)nt * nbatch, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    cudaFreeAsync(d_u0, ctx->stream);
+    cudaFreeAsync(d_ph, ctx->stream);
+    cudaFreeAsync(d_J, ctx->stream);
+    cudaFreeAsync(d_g, ctx->stream);
+    cudaFreeAsync(d_m, ctx->stream);
+    CU(cudaStreamSynchronize(ctx->stream));
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+// fl_fft.cuh -- block-wide Stockham FFT for one CTA, sm_100a.
+//
+// A length-N transform (N = T*E) is held E elements per thread: thread t owns
+// the samples/bins {t + s*T : s in [0, E)}.  The transform runs as radix-E
+// Stockham passes (plus one smaller-radix pass when log2 E does not divide
+// log2 N).  Inputs of the first pass and outputs of the last pass sit in the
+// same registers with the same ownership, so a forward transform, a pointwise
+// operation and an inverse transform never need a reorder pass; only the
+// passes in between exchange data through one padded shared-memory buffer.
+//
+// Conventions match FFTW as used by the reference: the forward transform is
+// unnormalised with exponent sign -1; the "inverse" here is the unnormalised
+// sign +1 transform (callers fold the 1/N of ifft into their pointwise step).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fl {
+
+template <typename R>
+struct __align__(2 * sizeof(R)) cx {
+    R re, im;
+};
+
+template <typename R>
+__device__ __forceinline__ cx<R> mk(R a, R b) {
+    cx<R> z;
+    z.re = a;
+    z.im = b;
+    return z;
+}
+template <typename R>
+__device__ __forceinline__ cx<R> operator+(cx<R> a, cx<R> b) { return mk(a.re + b.re, a.im + b.im); }
+template <typename R>
+__device__ __forceinline__ cx<R> operator-(cx<R> a, cx<R> b) { return mk(a.re - b.re, a.im - b.im); }
+template <typename R>
+__device__ __forceinline__ cx<R> cmul(cx<R> a, cx<R> b) {
+    return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+template <typename R>
+__device__ __forceinline__ cx<R> cmulc(cx<R> a, cx<R> b) {  // a * conj(b)
+    return mk(a.re * b.re + a.im * b.im, a.im * b.re - a.re * b.im);
+}
+template <typename R>
+__device__ __forceinline__ cx<R> scale(cx<R> a, R s) { return mk(a.re * s, a.im * s); }
+template <typename R>
+__device__ __forceinline__ cx<R> conjc(cx<R> a) { return mk(a.re, -a.im); }
+template <typename R>
+__device__ __forceinline__ R abs2(cx<R> a) { return a.re * a.re + a.im * a.im; }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename R>
+__device__ __forceinline__ cx<R> rot90(cx<R> a) {
+    return INV ? mk(-a.im, a.re) : mk(a.im, -a.re);
+}
+
+// padded shared-memory index: one pad element every 16 keeps the stride-16
+// writes of the first pass conflict-free for 8- and 16-byte elements
+__device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+__host__ __device__ constexpr int padded_len(int n) { return n + (n >> 4); }
+
+// exp(-2 pi i k/32) for k = 0..15: (cos, -sin) at multiples of pi/16
+// (literal values of the elementary constants).
+template <typename R>
+__device__ __forceinline__ cx<R> w32(int k) {
+    constexpr double C[16] = {1.0,
+                              0.98078528040323043058,
+                              0.92387953251128673848,
+                              0.83146961230254523567,
+                              0.70710678118654752440,
+                              0.55557023301960222474,
+                              0.38268343236508977173,
+                              0.19509032201612826785,
+                              0.0,
+                              -0.19509032201612826785,
+                              -0.38268343236508977173,
+                              -0.55557023301960222474,
+                              -0.70710678118654752440,
+                              -0.83146961230254523567,
+                              -0.92387953251128673848,
+                              -0.98078528040323043058};
+    // sin(pi k/16) = cos(pi (8 - k)/16) for k <= 8, = cos(pi (k - 8)/16) beyond
+    const double c = C[k];
+    const double s = k <= 8 ? C[8 - k] : C[k - 8];
+    return mk<R>(R(c), R(-s));
+}
+
+// multiply by exp(-+2 pi i k / 32) with the trivial cases special-cased
+template <bool INV, typename R>
+__device__ __forceinline__ cx<R> tw32(cx<R> a, int k) {
+    if (k == 0) return a;
+    if (k == 8) return rot90<INV>(a);
+    cx<R> w = w32<R>(k);
+    if (INV) w.im = -w.im;
+    return cmul(a, w);
+}
+
+// In-register radix-RAD DFT on a[base + STRIDE*r], r in [0, RAD):
+// radix-2 decimation-in-frequency stages, output de-scrambled by register
+// renaming (bit reversal of a compile-time index).  Loops are fully unrolled
+// so every index is a compile-time constant.
+template <int RAD, bool INV, int STRIDE, typename R, int E>
+__device__ __forceinline__ void dft_inreg(cx<R> (&a)[E], const int base) {
+    static_assert(RAD == 1 || RAD == 2 || RAD == 4 || RAD == 8 || RAD == 16 || RAD == 32,
+                  "radix");
+    if constexpr (RAD >= 2) {
+#pragma unroll
+        for (int half = RAD / 2; half >= 1; half >>= 1) {
+#pragma unroll
+            for (int blk = 0; blk < RAD; blk += 2 * half) {
+#pragma unroll
+                for (int j = 0; j < half; j++) {
+                    cx<R> u = a[base + STRIDE * (blk + j)];
+                    cx<R> v = a[base + STRIDE * (blk + j + half)];
+                    a[base + STRIDE * (blk + j)] = u + v;
+                    // twiddle exp(-2 pi i j / (2 half)) = w32^(j * 32 / (2 half))
+                    a[base + STRIDE * (blk + j + half)] = tw32<INV>(u - v, j * (32 / (2 * half)));
+                }
+            }
+        }
+        constexpr int LG = RAD == 2 ? 1 : RAD == 4 ? 2 : RAD == 8 ? 3 : RAD == 16 ? 4 : 5;
+        cx<R> tmp[RAD];
+#pragma unroll
+        for (int r = 0; r < RAD; r++) tmp[r] = a[base + STRIDE * r];
+#pragma unroll
+        for (int r = 0; r < RAD; r++) {
+            int rv = 0;
+#pragma unroll
+            for (int b = 0; b < LG; b++)
+                if (r & (1 << b)) rv |= 1 << (LG - 1 - b);
+            a[base + STRIDE * r] = tmp[rv];
+        }
+    }
+}
+
+template <int LOGN, int LOGE>
+struct FftShape {
+    static constexpr int N = 1 << LOGN;
+    static constexpr int E = 1 << LOGE;
+    static constexpr int T = N / E;
+    static constexpr int NFULL = LOGN / LOGE;       // full radix-E passes
+    static constexpr int REM = LOGN % LOGE;         // bits of the last pass
+    static constexpr int NPASS = NFULL + (REM > 0 ? 1 : 0);
+};
+
+// One Stockham pass p of radix RP with stride NS (= product of the previous
+// radices).  FIRST: inputs come from registers; LAST: outputs stay in
+// registers.  Between passes the data goes through the padded smem buffer.
+template <typename R, int LOGN, int LOGE, int RP, int NS, bool FIRST, bool LAST, bool INV>
+__device__ __forceinline__ void stockham_pass(cx<R> (&v)[1 << LOGE], cx<R>* __restrict__ sm,
+                                              const cx<R>* __restrict__ tw) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int E = S::E, T = S::T, N = S::N;
+    constexpr int BPT = E / RP;  // butterflies per thread
+    const int t = threadIdx.x;
+    if constexpr (!FIRST) {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = sm[pad(t + T * s)];
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < BPT; q++) {
+        const int j = t + T * q;
+        if constexpr (NS > 1) {
+            const int m = j & (NS - 1);
+            constexpr int TWS = N / (NS * RP);
+#pragma unroll
+            for (int r = 1; r < RP; r++) {
+                cx<R> w = tw[m * r * TWS];
+                if (INV) w.im = -w.im;
+                v[q + BPT * r] = cmul(v[q + BPT * r], w);
+            }
+        }
+        dft_inreg<RP, INV, BPT>(v, q);
+        if constexpr (!LAST) {
+            const int base = (j / NS) * NS * RP + (j & (NS - 1));
+#pragma unroll
+            for (int r = 0; r < RP; r++) sm[pad(base + r * NS)] = v[q + BPT * r];
+        }
+    }
+    if constexpr (!LAST) __syncthreads();
+}
+
+template <typename R, int LOGN, int LOGE, bool INV, int P>
+__device__ __forceinline__ void fft_passes(cx<R> (&v)[1 << LOGE], cx<R>* sm, const cx<R>* tw) {
+    using S = FftShape<LOGN, LOGE>;
+    if constexpr (P < S::NPASS) {
+        constexpr int RP = (P < S::NFULL) ? S::E : (1 << S::REM);
+        constexpr int NS = 1 << (LOGE * P);
+        stockham_pass<R, LOGN, LOGE, RP, NS, P == 0, P == S::NPASS - 1, INV>(v, sm, tw);
+        fft_passes<R, LOGN, LOGE, INV, P + 1>(v, sm, tw);
+    }
+}
+
+// Block-wide unnormalised transform of the N values held in v (all threads
+// of the block must call it).  The smem buffer must hold padded_len(N)
+// elements and must not be in use by the caller across this call.
+template <typename R, int LOGN, int LOGE, bool INV>
+__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], cx<R>* sm, const cx<R>* tw) {
+    fft_passes<R, LOGN, LOGE, INV, 0>(v, sm, tw);
+}
+
+}  // namespace fl

@@ -1,0 +1,886 @@
+// fl_sm.cuh -- single-mode GMMNLSE stepper: one CTA owns one problem (slot)
+// and runs its whole adaptive Tsit5 solve, the checkpoint-replay recompute
+// and the adjoint solve as a state machine whose state lives in global
+// memory, so a launch can advance a slot by a bounded number of attempted
+// steps (serving) or run it to completion (plain drop-in).
+//
+// Reference path: forward RHS src/simulation/simulate_disp_mmf.jl:25-60,
+// adjoint RHS src/simulation/sensitivity_disp_mmf.jl:32-79 (with the helper
+// terms :93-215), drivers simulate_disp_mmf.jl:183-207 and
+// sensitivity_disp_mmf.jl:309-332, band objective
+// src/fiberlab/physics_helpers.jl:222-232, phase gradient
+// src/fiberlab/physics_models.jl:1042.
+//
+// For M = 1 the RHS is evaluated in an algebraically identical form with
+// fewer transforms (4 forward, 5 adjoint instead of 4 and 14):
+//   forward  dũ = i e^{-iDz} τ F⁻¹[((1-fR) I + h∗I) u_t],  I = γ|u_t|²
+//   adjoint  dλ̃ = i e^{-iDz} F⁻¹[ λ_t (2(1-fR) I + h∗I) - (1-fR) γ λ_t* u_t²
+//                                 + 2i (h̃⋆Y) u_t ],  Y = γ Im(λ_t u_t*)
+// where u_t = F(e^{iDz} ũ), λ_t = F(e^{iDz} τ λ̃), h∗ is the Raman convolution
+// with the fftshift folded into Heff = hR (-1)^k, and h̃⋆ the correlation
+// (conj(Heff)).  The two Raman terms of the reference adjoint (:93-132) are
+// complex conjugates of each other and combine into the single real
+// correlation of Y; h∗I and h̃⋆Y share one complex transform pair.
+#pragma once
+#include "fl_fft.cuh"
+#include "fl_types.h"
+
+namespace fl {
+
+// Tsitouras (2011) 5(4) pair, as used by OrdinaryDiffEq's Tsit5.
+static __device__ __constant__ double kT5c[7] = {0.0, 0.161, 0.327, 0.9, 0.9800255409045097, 1.0, 1.0};
+static __device__ __constant__ double kT5a[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {0.161, 0, 0, 0, 0, 0},
+    {-0.008480655492356989, 0.335480655492357, 0, 0, 0, 0},
+    {2.897153057105493, -6.359448489975075, 4.3622954328695815, 0, 0, 0},
+    {5.325864828439257, -11.748883564062828, 7.4955393428898365, -0.09249506636175525, 0, 0},
+    {5.86145544294642, -12.92096931784711, 8.159367898576159, -0.071584973281401,
+     -0.028269050394068383, 0},
+    {0.09646076681806523, 0.01, 0.4798896504144996, 1.379008574103742, -3.290069515436081,
+     2.324710524099774}};
+static __device__ __constant__ double kT5bt[7] = {-0.00178001105222577714, -0.0008164344596567469,
+                                           0.007880878010261995,    -0.1447110071732629,
+                                           0.5823571654525552,      -0.45808210592918697,
+                                           0.015151515151515152};
+// free 4th-order interpolant b_i(θ) = Σ_p r[i][p] θ^(p+1)
+static __device__ __constant__ double kT5r[7][4] = {
+    {1.0, -2.763706197274826, 2.9132554618219126, -1.0530884977290216},
+    {0.0, 0.13169999999999998, -0.2234, 0.1017},
+    {0.0, 3.9302962368947516, -5.941033872131505, 2.490627285651253},
+    {0.0, -12.411077166933676, 30.33818863028232, -16.548102889244902},
+    {0.0, 37.50931341651104, -88.1789048947664, 47.37952196281928},
+    {0.0, -27.896526289197286, 65.09189467479366, -34.87065786149661},
+    {0.0, 1.5, -4.0, 2.5}};
+
+// PI controller defaults of OrdinaryDiffEq for a 5th-order method
+constexpr double kBeta1 = 7.0 / 50.0, kBeta2 = 2.0 / 25.0, kGamma = 0.9;
+constexpr double kQmin = 0.2, kQmax = 10.0, kQoldInit = 1e-4;
+constexpr double kEps = 2.220446049250313e-16;
+
+// exp(+i D z) from the FP64 phase in turns reduced to [-1/2, 1/2] before the
+// sincos of the working precision.
+template <typename R>
+__device__ __forceinline__ cx<R> phasor(double dturn, double z);
+template <>
+__device__ __forceinline__ cx<float> phasor<float>(double dturn, double z) {
+    double ph = dturn * z;
+    ph -= rint(ph);
+    float s, c;
+    sincospif(2.0f * (float)ph, &s, &c);
+    return mk(c, s);
+}
+template <>
+__device__ __forceinline__ cx<double> phasor<double>(double dturn, double z) {
+    double ph = dturn * z;
+    ph -= rint(ph);
+    double s, c;
+    sincospi(2.0 * ph, &s, &c);
+    return mk(c, s);
+}
+
+__device__ __forceinline__ cx<double> ld2(const double* p, int b) {
+    const double2 v = reinterpret_cast<const double2*>(p)[b];
+    return mk(v.x, v.y);
+}
+__device__ __forceinline__ void st2(double* p, int b, cx<double> v) {
+    reinterpret_cast<double2*>(p)[b] = make_double2(v.re, v.im);
+}
+template <typename R>
+__device__ __forceinline__ cx<double> up(cx<R> a) {
+    return mk((double)a.re, (double)a.im);
+}
+template <typename R>
+__device__ __forceinline__ cx<R> down(cx<double> a) {
+    return mk((R)a.re, (R)a.im);
+}
+
+// deterministic block reductions (fixed shuffle tree, fixed warp order)
+template <int T>
+__device__ __forceinline__ double block_sum(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < T / 32; w++) s += red[w];
+    return s;
+}
+template <int T>
+__device__ __forceinline__ double block_max(double v, double* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+#pragma unroll
+    for (int w = 0; w < T / 32; w++) s = fmax(s, red[w]);
+    return s;
+}
+
+template <typename R, int LOGN, int LOGE>
+struct SmSolver {
+    using S = FftShape<LOGN, LOGE>;
+    static constexpr int N = S::N, E = S::E, T = S::T;
+    using C = cx<R>;
+
+    const SlotDesc<R>& d;
+    C* sm;          // padded transform buffer
+    double* red;    // 32 doubles
+    const C* tw;
+    const C* Heff;
+    const R* ss;
+    C* scr0;
+    C* scr1;
+
+    __device__ SmSolver(const SlotDesc<R>& dd, C* smem, double* r)
+        : d(dd), sm(smem), red(r), tw((const C*)dd.tw), Heff((const C*)dd.Heff),
+          ss((const R*)dd.ss), scr0((C*)dd.scr[0]), scr1((C*)dd.scr[1]) {}
+
+    __device__ __forceinline__ static int bin(int s) { return threadIdx.x + T * s; }
+
+    // forward RHS: v holds the stage input ũ (own bins) and receives dũ/dz
+    __device__ void rhs_fwd(double z, C (&v)[E]) {
+        const R g = (R)d.gamma, ofr = (R)d.one_m_fR, invn = R(1) / R(N);
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
+        block_fft<R, LOGN, LOGE, false>(v, sm, tw);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            scr0[bin(s)] = v[s];
+            v[s] = mk(g * abs2(v[s]), R(0));
+        }
+        block_fft<R, LOGN, LOGE, false>(v, sm, tw);
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = cmul(v[s], Heff[bin(s)]);
+        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const C ut = scr0[bin(s)];
+            const R f = ofr * (g * abs2(ut)) + v[s].re * invn;
+            v[s] = scale(ut, f);
+        }
+        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            const C y = cmulc(v[s], phasor<R>(d.Dturns[b], z));  // e^{-iDz} x
+            const R sc = ss[b] * invn;
+            v[s] = mk(-y.im * sc, y.re * sc);                      // i * y * τ / N
+        }
+    }
+
+    // adjoint RHS: v holds the stage input λ̃ and receives dλ̃/dz; load_u(v)
+    // fills v with the forward field ũ(z) (one register array at a time)
+    template <class LoadU>
+    __device__ void rhs_adj(double z, C (&v)[E], LoadU&& load_u) {
+        const R g = (R)d.gamma, ofr = (R)d.one_m_fR, invn = R(1) / R(N);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            v[s] = scale(cmul(v[s], phasor<R>(d.Dturns[b], z)), ss[b]);
+        }
+        block_fft<R, LOGN, LOGE, false>(v, sm, tw);   // λ_t
+#pragma unroll
+        for (int s = 0; s < E; s++) scr0[bin(s)] = v[s];
+        load_u(v);
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
+        block_fft<R, LOGN, LOGE, false>(v, sm, tw);   // u_t
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            const C lt = scr0[b];
+            scr1[b] = v[s];
+            const R I = g * abs2(v[s]);
+            const R Y = g * (lt.im * v[s].re - lt.re * v[s].im);  // γ Im(λ u*)
+            v[s] = mk(I, Y);
+        }
+        block_fft<R, LOGN, LOGE, false>(v, sm, tw);
+        // split the two real spectra: X[k] and conj(X[-k])
+#pragma unroll
+        for (int s = 0; s < E; s++) sm[pad(bin(s))] = v[s];
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            const C zm = conjc(sm[pad((N - b) & (N - 1))]);
+            const C H = Heff[b];
+            const C a = scale(v[s] + zm, R(0.5));   // spectrum of I
+            const C c = scale(v[s] - zm, R(0.5));   // i * spectrum of Y
+            v[s] = cmul(a, H) + cmulc(c, H);
+        }
+        __syncthreads();
+        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            const C lt = scr0[b], ut = scr1[b];
+            const R I = g * abs2(ut);
+            const R Rr = v[s].re * invn, Ri = v[s].im * invn;
+            const C t1 = scale(lt, R(2) * ofr * I + Rr);
+            const C u2 = cmul(ut, ut);
+            const C t2 = scale(cmulc(u2, lt), ofr * g);      // (1-fR) γ conj(λ) u²
+            const C t3 = mk(-R(2) * Ri * ut.im, R(2) * Ri * ut.re);  // 2i Ri u
+            v[s] = t1 - t2 + t3;
+        }
+        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const C y = cmulc(v[s], phasor<R>(d.Dturns[bin(s)], z));
+            v[s] = mk(-y.im * invn, y.re * invn);
+        }
+    }
+
+    // ---- stage helpers ---------------------------------------------------
+    __device__ __forceinline__ static C* kp(void* const (&k)[7], int perm, int i) {
+        // logical stage i -> physical buffer; perm swaps stages 0 and 6 (FSAL)
+        int p = (perm && (i == 0 || i == 6)) ? 6 - i : i;
+        return (C*)k[p];
+    }
+
+    // v = ũ_n + dt Σ_{j<st} a[st][j] k_j   (FP64 accumulation)
+    __device__ __forceinline__ void stage_input(int st, const double* u, void* const (&k)[7],
+                                                int perm, double dt, C (&v)[E]) {
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            double ar = 0.0, ai = 0.0;
+            for (int j = 0; j < st; j++) {
+                const C kj = kp(k, perm, j)[b];
+                const double a = kT5a[st][j];
+                ar += a * (double)kj.re;
+                ai += a * (double)kj.im;
+            }
+            const cx<double> un = ld2(u, b);
+            v[s] = mk((R)(un.re + dt * ar), (R)(un.im + dt * ai));
+        }
+    }
+
+    // stage 7 input = ũ_{n+1} (written to unew in FP64), partial error
+    // dt Σ_{j<7} b̃_j k_j and the weights abstol + reltol max(|u_n|,|u_{n+1}|)
+    __device__ __forceinline__ void stage7_input(const double* u, double* unew,
+                                                 void* const (&k)[7], int perm, double dt,
+                                                 double abstol, double reltol, C (&v)[E],
+                                                 bool want_err) {
+        C* esv = (C*)d.esv;
+        R* skv = (R*)d.skv;
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
+            for (int j = 0; j < 6; j++) {
+                const C kj = kp(k, perm, j)[b];
+                const double a = kT5a[6][j], bt = kT5bt[j];
+                ar += a * (double)kj.re;
+                ai += a * (double)kj.im;
+                er += bt * (double)kj.re;
+                ei += bt * (double)kj.im;
+            }
+            const cx<double> un = ld2(u, b);
+            const cx<double> u1 = mk(un.re + dt * ar, un.im + dt * ai);
+            st2(unew, b, u1);
+            if (want_err) {
+                esv[b] = mk((R)(dt * er), (R)(dt * ei));
+                const double m0 = sqrt(un.re * un.re + un.im * un.im);
+                const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
+                skv[b] = (R)(abstol + fmax(m0, m1) * reltol);
+            }
+            v[s] = down<R>(u1);
+        }
+    }
+
+    // finish the error estimate with k7 (in v) -> EEst (block-uniform)
+    __device__ __forceinline__ double error_norm(const C (&k7)[E], double dt) {
+        const C* esv = (const C*)d.esv;
+        const R* skv = (const R*)d.skv;
+        const double bt7 = kT5bt[6];
+        double acc = 0.0;
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            const C e6 = esv[b];
+            const double er = (double)e6.re + dt * bt7 * (double)k7[s].re;
+            const double ei = (double)e6.im + dt * bt7 * (double)k7[s].im;
+            const double w = 1.0 / (double)skv[b];
+            acc += (er * er + ei * ei) * (w * w);
+        }
+        const double tot = block_sum<T>(acc, red);
+        return sqrt(tot / (double)N);
+    }
+
+    // dense interpolant of a stored forward step at θ, into w
+    __device__ __forceinline__ void interp(int slot, double dtn, double th, C (&w)[E]) {
+        const C* sg = (const C*)d.seg + (size_t)slot * 5 * N;
+        const double t2 = th * th, t3 = t2 * th, t4 = t3 * th;
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = bin(s);
+            const C c0 = sg[b], c1 = sg[N + b], c2 = sg[2 * N + b], c3 = sg[3 * N + b],
+                    c4 = sg[4 * N + b];
+            const double xr = (double)c0.re + dtn * (th * (double)c1.re + t2 * (double)c2.re +
+                                                     t3 * (double)c3.re + t4 * (double)c4.re);
+            const double xi = (double)c0.im + dtn * (th * (double)c1.im + t2 * (double)c2.im +
+                                                     t3 * (double)c3.im + t4 * (double)c4.im);
+            w[s] = mk((R)xr, (R)xi);
+        }
+    }
+};
+
+// PI controller: returns q and q11 (OrdinaryDiffEqCore stepsize_controller!)
+__device__ __forceinline__ double pi_q(double EEst, double qold, double& q11) {
+    if (EEst == 0.0) {
+        q11 = 0.0;
+        return 1.0 / kQmax;
+    }
+    q11 = pow(EEst, kBeta1);
+    double q = q11 / pow(qold, kBeta2);
+    q = q / kGamma;
+    return fmax(1.0 / kQmax, fmin(1.0 / kQmin, q));
+}
+
+// Hairer initial step from the norms of the launch, f0 and the probe f1
+// (OrdinaryDiffEqCore ode_determine_initdt; 5 = the method order).
+__device__ __forceinline__ double initdt_first(double d0, double d1, double span) {
+    double dt0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : (d0 / d1) / 100.0;
+    return fmin(dt0, span);
+}
+__device__ __forceinline__ double initdt_final(double dt0, double d1, double d2, double nd,
+                                               double dtmin, double span) {
+    if (nd == 0.0) return fmax(dtmin, 100 * dt0);  // constant derivative over the probe
+    const double mx = fmax(d1, d2);
+    const double dt1 = mx <= 1e-15 ? fmax(1e-6, dt0 * 1e-3) : pow(10.0, -(2.0 + log10(mx)) / 5.0);
+    return fmax(dtmin, fmin(fmin(100 * dt0, dt1), span));
+}
+
+template <typename R, int LOGN, int LOGE>
+struct SegLoader {
+    using Sol = SmSolver<R, LOGN, LOGE>;
+    Sol& S;
+    int seg_lo, seg_hi;
+    double zz;
+    __device__ void operator()(cx<R> (&w)[Sol::E]) const {
+        const double* lg = S.d.steplog;
+        int n = seg_lo;
+        while (n + 1 < seg_hi && lg[2 * (n + 1)] <= zz) n++;
+        const double zn = lg[2 * n], dtn = lg[2 * n + 1];
+        S.interp(n - seg_lo, dtn, (zz - zn) / dtn, w);
+    }
+};
+
+template <typename R, int LOGN, int LOGE>
+__device__ __forceinline__ void restore_checkpoint(const SlotDesc<R>& d, int seg, SlotState& st) {
+    using Sol = SmSolver<R, LOGN, LOGE>;
+    using C = cx<R>;
+    constexpr int N = Sol::N, E = Sol::E;
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int b = Sol::bin(s);
+        reinterpret_cast<double2*>(d.u[0])[b] =
+            reinterpret_cast<const double2*>(d.ck_u)[(size_t)seg * N + b];
+        ((C*)d.kf[0])[b] = ((const C*)d.ck_k1)[(size_t)seg * N + b];
+    }
+    st.cur = 0;
+    st.kperm = 0;
+    st.rec_pos = 0;
+    st.stage = 0;
+}
+
+template <typename R, int LOGN, int LOGE>
+__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+    sm_advance_kernel(const SlotDesc<R>* __restrict__ descs, SlotState* __restrict__ states,
+                      const int* __restrict__ active, int max_evals) {
+    using Sol = SmSolver<R, LOGN, LOGE>;
+    using C = cx<R>;
+    constexpr int N = Sol::N, E = Sol::E, T = Sol::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    double* red = reinterpret_cast<double*>(smraw + sizeof(C) * padded_len(N));
+
+    const int slot = active[blockIdx.x];
+    const SlotDesc<R>& d = descs[slot];
+    SlotState st = states[slot];  // block-uniform copy
+    Sol S(d, sm, red);
+    const int tid = threadIdx.x;
+    const double L = d.L, dtmin = kEps * L;
+    C v[E];
+    int evals = 0;
+
+    while (st.phase != PH_DONE && evals < max_evals) {
+        // ------------------------------------------------ phases without an RHS
+        if (st.phase == PH_SEED) {
+            // terminal seed λ̃(L) (interaction frame) into lam[0]
+            const double* uf = d.u[st.cur];
+            double* lam = d.lam[0];
+            if (d.mode == MODE_BAND_GRADIENT) {
+                double et = 0.0, eb = 0.0;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    const cx<double> x = ld2(uf, b);
+                    const double e = x.re * x.re + x.im * x.im;
+                    et += e;
+                    if (d.mask[b]) eb += e;
+                }
+                const double tot = block_sum<T>(et, red);
+                const double band = block_sum<T>(eb, red);
+                const double cost = band / tot;
+                double sc = 1.0 / tot;
+                st.J = cost;
+                if (d.log_cost) {  // physics_helpers.jl:320-326
+                    st.J = 10.0 * log10(fmax(cost, 1e-15));
+                    sc *= cost <= 1e-15 ? 0.0 : 10.0 / (log(10.0) * cost);
+                }
+                // e^{-iDL} (u_L (mask - J)/E) = ũ(L) (mask - J)/E
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    const cx<double> x = ld2(uf, b);
+                    const double f = ((d.mask[b] ? 1.0 : 0.0) - cost) * sc;
+                    st2(lam, b, mk(x.re * f, x.im * f));
+                }
+            } else {
+                st.J = 0.0;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    const cx<double> x = ld2(d.lamL, b);
+                    const cx<double> p = phasor<double>(d.Dturns[b], L);
+                    st2(lam, b, mk(x.re * p.re + x.im * p.im, x.im * p.re - x.re * p.im));
+                }
+            }
+            double mx = 0.0;
+            bool finite = true;
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const cx<double> x = ld2(lam, Sol::bin(s));
+                const double a = sqrt(x.re * x.re + x.im * x.im);
+                if (!isfinite(a)) finite = false;
+                mx = fmax(mx, a);
+            }
+            const double scl = block_max<T>(finite ? mx : INFINITY, red);
+            if (!isfinite(scl)) {
+                st.status = ST_NONFINITE;
+                st.phase = PH_DONE;
+                continue;
+            }
+            st.abstol_adj = scl == 0.0 ? d.abstol : d.abstol * scl;  // sensitivity_disp_mmf.jl:324-325
+            if (st.ck_stride > d.seg_cap) {
+                st.status = ST_CAPACITY;
+                st.phase = PH_DONE;
+                continue;
+            }
+            st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
+            st.acur = 0;
+            st.akperm = 0;
+            st.a_naccept = st.a_nreject = st.a_nf = st.a_iters = 0;
+            restore_checkpoint<R, LOGN, LOGE>(d, st.seg, st);
+            st.phase = PH_REC;
+            continue;
+        }
+        if (st.phase == PH_FINAL) {
+            // λ(0) = λ̃(0); ∂J/∂φ = 2 Re(conj(λ0) i u_shaped) (physics_models.jl:1042)
+            const double* lam = d.lam[st.acur];
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int b = Sol::bin(s);
+                const cx<double> l = ld2(lam, b);
+                if (d.lam0_out) st2(d.lam0_out, b, l);
+                if (d.grad_out) {
+                    const cx<double> us = ld2(d.u0, b);
+                    d.grad_out[b] = 2.0 * (l.im * us.re - l.re * us.im);
+                }
+            }
+            st.phase = PH_DONE;
+            continue;
+        }
+
+        // ------------------------------------------------ build the stage input
+        const bool adj = st.phase == PH_ADJ_INIT || st.phase == PH_ADJ;
+        double ze = 0.0, zload = 0.0;
+        if (st.phase == PH_FWD_INIT) {
+            const C* k1 = (const C*)d.kf[0];
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int b = Sol::bin(s);
+                const cx<double> x = ld2(d.u0, b);
+                if (st.stage == 0) {
+                    st2(d.u[0], b, x);
+                    v[s] = down<R>(x);
+                } else {
+                    const C f0 = k1[b];
+                    v[s] = mk((R)(x.re + st.cdt * (double)f0.re), (R)(x.im + st.cdt * (double)f0.im));
+                }
+            }
+            ze = st.stage == 0 ? 0.0 : st.cdt;
+        } else if (st.phase == PH_FWD || st.phase == PH_REC) {
+            if (st.stage == 0) {
+                if (st.phase == PH_REC) {
+                    const int n = st.seg * st.ck_stride + st.rec_pos;
+                    st.cz = d.steplog[2 * n];
+                    st.cdt = d.steplog[2 * n + 1];
+                } else {
+                    if (++st.iters > d.max_iters) {
+                        st.status = ST_MAXITERS;
+                        st.phase = PH_DONE;
+                        continue;
+                    }
+                    // fix_dt_at_bounds!, modify_dt_for_tstops!
+                    double adt = fmax(fmin(fabs(st.dt), L), dtmin);
+                    const double rem = L - st.z;
+                    if (adt > rem) adt = rem;
+                    if (adt <= dtmin && rem > dtmin) {
+                        st.status = ST_DT_UNDERFLOW;
+                        st.phase = PH_DONE;
+                        continue;
+                    }
+                    st.cz = st.z;
+                    st.cdt = adt;
+                }
+                st.stage = 1;
+            }
+            const double* u = d.u[st.cur];
+            if (st.stage < 6)
+                S.stage_input(st.stage, u, d.kf, st.kperm, st.cdt, v);
+            else
+                S.stage7_input(u, d.u[st.cur ^ 1], d.kf, st.kperm, st.cdt, d.abstol, d.reltol, v,
+                               st.phase == PH_FWD);
+            ze = st.cz + kT5c[st.stage] * st.cdt;
+        } else if (st.phase == PH_ADJ_INIT) {
+            const double* lam = d.lam[0];
+            const C* k1 = (const C*)d.ka[0];
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int b = Sol::bin(s);
+                const cx<double> x = ld2(lam, b);
+                if (st.stage == 0) {
+                    v[s] = down<R>(x);
+                } else {
+                    const C f0 = k1[b];
+                    v[s] = mk((R)(x.re - st.cdt * (double)f0.re), (R)(x.im - st.cdt * (double)f0.im));
+                }
+            }
+            ze = st.stage == 0 ? L : L - st.cdt;
+            zload = st.stage == 0 ? L : fmax(ze, d.steplog[2 * (st.seg * st.ck_stride)]);
+        } else {  // PH_ADJ
+            const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
+            if (st.stage == 0) {
+                if (++st.a_iters > d.max_iters) {
+                    st.status = ST_MAXITERS;
+                    st.phase = PH_DONE;
+                    continue;
+                }
+                double adt = fmax(fmin(fabs(st.adt), L), dtmin);
+                const double rem = st.az - zlo;
+                if (adt > rem) adt = rem;
+                st.cz = st.az;
+                st.cdt = -adt;
+                st.stage = 1;
+            }
+            const double* lam = d.lam[st.acur];
+            if (st.stage < 6)
+                S.stage_input(st.stage, lam, d.ka, st.akperm, st.cdt, v);
+            else
+                S.stage7_input(lam, d.lam[st.acur ^ 1], d.ka, st.akperm, st.cdt, st.abstol_adj,
+                               d.reltol, v, true);
+            ze = zload = st.cz + kT5c[st.stage] * st.cdt;
+        }
+
+        // ------------------------------------------------ one RHS evaluation
+        if (adj) {
+            const int seg_lo = st.seg * st.ck_stride;
+            const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
+            SegLoader<R, LOGN, LOGE> ld{S, seg_lo, seg_hi, zload};
+            S.rhs_adj(ze, v, ld);
+        } else {
+            S.rhs_fwd(ze, v);
+        }
+        evals++;
+
+        // ------------------------------------------------ consume the derivative
+        if (st.phase == PH_FWD_INIT || st.phase == PH_ADJ_INIT) {
+            const bool fw = st.phase == PH_FWD_INIT;
+            const double* x0 = fw ? d.u0 : d.lam[0];
+            const double at = fw ? d.abstol : st.abstol_adj, rt = d.reltol;
+            C* k1 = (C*)(fw ? d.kf[0] : d.ka[0]);
+            if (st.stage == 0) {
+                double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    k1[b] = v[s];
+                    const cx<double> x = ld2(x0, b);
+                    const double ax = sqrt(x.re * x.re + x.im * x.im);
+                    const double sk = at + ax * rt;
+                    s0 += (ax / sk) * (ax / sk);
+                    const double af = sqrt(abs2(up(v[s])));
+                    s1 += (af / sk) * (af / sk);
+                }
+                const double d0 = sqrt(block_sum<T>(s0, red) / N);
+                const double d1 = sqrt(block_sum<T>(s1, red) / N);
+                const double dt0 = initdt_first(d0, d1, L);
+                double dtinit = -1.0;
+                if (!isfinite(d1)) dtinit = dtmin;
+                else if (dt0 < 10 * kEps) dtinit = fmax(1e-6, dtmin);
+                if (dtinit < 0.0) {
+                    st.cdt = dt0;  // probe step
+                    st.cz = d1;
+                    st.stage = 1;
+                    continue;
+                }
+                st.cdt = dtinit;
+            } else {
+                double s2 = 0.0, ndiff = 0.0;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    const cx<double> x = ld2(x0, b);
+                    const double sk = at + sqrt(x.re * x.re + x.im * x.im) * rt;
+                    const C f0 = k1[b];
+                    const double dr = (double)v[s].re - (double)f0.re;
+                    const double di = (double)v[s].im - (double)f0.im;
+                    s2 += (dr * dr + di * di) / (sk * sk);
+                    ndiff += (dr != 0.0 || di != 0.0) ? 1.0 : 0.0;
+                }
+                const double d2 = sqrt(block_sum<T>(s2, red) / N) / st.cdt;
+                const double nd = block_sum<T>(ndiff, red);
+                st.cdt = initdt_final(st.cdt, st.cz, d2, nd, dtmin, L);
+            }
+            st.stage = 0;
+            if (fw) {
+                st.z = 0.0;
+                st.dt = st.cdt;
+                st.qold = kQoldInit;
+                st.cur = 0;
+                st.kperm = 0;
+                st.nsteps = 0;
+                st.ck_stride = 1;
+                st.naccept = st.nreject = st.iters = 0;
+                st.nf = 3;
+                if (d.ck_cap > 0) {
+#pragma unroll
+                    for (int s = 0; s < E; s++) {
+                        const int b = Sol::bin(s);
+                        reinterpret_cast<double2*>(d.ck_u)[b] =
+                            reinterpret_cast<const double2*>(d.u0)[b];
+                        ((C*)d.ck_k1)[b] = k1[b];
+                    }
+                }
+                st.save_idx = 0;
+                while (st.save_idx < d.nsave && d.zsave[st.save_idx] == 0.0) {
+                    double* o = d.save_out + (size_t)st.save_idx * 2 * N;
+#pragma unroll
+                    for (int s = 0; s < E; s++) st2(o, Sol::bin(s), ld2(d.u0, Sol::bin(s)));
+                    st.save_idx++;
+                }
+                st.phase = PH_FWD;
+            } else {
+                st.az = L;
+                st.adt = -st.cdt;
+                st.aqold = kQoldInit;
+                st.a_nf = 3;
+                st.acur = 0;
+                st.akperm = 0;
+                st.phase = PH_ADJ;
+            }
+            continue;
+        }
+
+        if (st.phase == PH_FWD || st.phase == PH_REC) {
+            const bool rec = st.phase == PH_REC;
+            C* ko = Sol::kp(d.kf, st.kperm, st.stage);
+#pragma unroll
+            for (int s = 0; s < E; s++) ko[Sol::bin(s)] = v[s];
+            if (st.stage < 6) {
+                st.stage++;
+                continue;
+            }
+            st.stage = 0;
+            const double z = st.cz, dt = st.cdt;
+            const double* u = d.u[st.cur];
+            if (rec) {
+                // interpolant of this step: c0 = ũ_n, c_p = Σ_i r_ip k_i
+                C* sg = (C*)d.seg + (size_t)st.rec_pos * 5 * N;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    sg[b] = down<R>(ld2(u, b));
+                    double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+                    for (int i = 0; i < 7; i++) {
+                        const C ki = Sol::kp(d.kf, st.kperm, i)[b];
+#pragma unroll
+                        for (int q = 0; q < 4; q++) {
+                            cr[q] += kT5r[i][q] * (double)ki.re;
+                            ci[q] += kT5r[i][q] * (double)ki.im;
+                        }
+                    }
+#pragma unroll
+                    for (int q = 0; q < 4; q++) sg[(q + 1) * N + b] = mk((R)cr[q], (R)ci[q]);
+                }
+                st.cur ^= 1;
+                st.kperm ^= 1;
+                st.rec_pos++;
+                const int seg_lo = st.seg * st.ck_stride;
+                if (seg_lo + st.rec_pos >= min(seg_lo + st.ck_stride, st.nsteps))
+                    st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
+                continue;
+            }
+            const double EEst = S.error_norm(v, dt);
+            if (!isfinite(EEst)) {
+                st.status = ST_NONFINITE;
+                st.phase = PH_DONE;
+                continue;
+            }
+            double q11;
+            const double q = pi_q(EEst, st.qold, q11);
+            st.nf += 6;
+            if (EEst > 1.0) {
+                st.nreject++;
+                st.dt = dt / fmin(1.0 / kQmin, q11 / kGamma);
+                continue;
+            }
+            st.naccept++;
+            if (st.nsteps >= d.step_cap) {
+                st.status = ST_CAPACITY;
+                st.phase = PH_DONE;
+                continue;
+            }
+            if (tid == 0) {
+                d.steplog[2 * st.nsteps] = z;
+                d.steplog[2 * st.nsteps + 1] = dt;
+            }
+            double znew = z + dt;
+            if (fabs(znew - L) < 100.0 * kEps * fmax(z, L)) znew = L;  // snap to the tstop
+            // save positions strictly inside (z, znew): dense output
+            while (st.save_idx < d.nsave && d.zsave[st.save_idx] < znew &&
+                   d.zsave[st.save_idx] > z) {
+                const double zs = d.zsave[st.save_idx];
+                const double th = (zs - z) / dt;
+                double* o = d.save_out + (size_t)st.save_idx * 2 * N;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    double xr = 0.0, xi = 0.0;
+                    for (int i = 0; i < 7; i++) {
+                        double bi = 0.0, tp = th;
+                        for (int qq = 0; qq < 4; qq++) {
+                            bi += kT5r[i][qq] * tp;
+                            tp *= th;
+                        }
+                        const C ki = Sol::kp(d.kf, st.kperm, i)[b];
+                        xr += bi * (double)ki.re;
+                        xi += bi * (double)ki.im;
+                    }
+                    const cx<double> un = ld2(u, b);
+                    const cx<double> x = mk(un.re + dt * xr, un.im + dt * xi);
+                    const cx<double> p = phasor<double>(d.Dturns[b], zs);
+                    st2(o, b, mk(x.re * p.re - x.im * p.im, x.re * p.im + x.im * p.re));
+                }
+                st.save_idx++;
+            }
+            st.nsteps++;
+            st.z = znew;
+            st.cur ^= 1;
+            st.kperm ^= 1;
+            st.qold = fmax(EEst, kQoldInit);
+            st.dt = fmin(fmax((q == 1.0) ? dt : dt / q, dtmin), L);
+            // z-checkpoints with thinning: K slots at steps j*stride
+            if (d.ck_cap > 0 && (st.nsteps % st.ck_stride) == 0) {
+                int slotc = st.nsteps / st.ck_stride;
+                if (slotc >= d.ck_cap) {
+                    for (int j = 1; j < d.ck_cap / 2; j++) {
+#pragma unroll
+                        for (int s = 0; s < E; s++) {
+                            const int b = Sol::bin(s);
+                            reinterpret_cast<double2*>(d.ck_u)[(size_t)j * N + b] =
+                                reinterpret_cast<double2*>(d.ck_u)[(size_t)2 * j * N + b];
+                            ((C*)d.ck_k1)[(size_t)j * N + b] = ((C*)d.ck_k1)[(size_t)2 * j * N + b];
+                        }
+                    }
+                    st.ck_stride *= 2;
+                    slotc = st.nsteps / st.ck_stride;
+                }
+                const double* un = d.u[st.cur];
+                const C* k1 = Sol::kp(d.kf, st.kperm, 0);
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    reinterpret_cast<double2*>(d.ck_u)[(size_t)slotc * N + b] =
+                        reinterpret_cast<const double2*>(un)[b];
+                    ((C*)d.ck_k1)[(size_t)slotc * N + b] = k1[b];
+                }
+            }
+            if (st.z == L) {
+                const double* uf = d.u[st.cur];
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = Sol::bin(s);
+                    const cx<double> x = ld2(uf, b);
+                    const cx<double> p = phasor<double>(d.Dturns[b], L);
+                    const cx<double> y = mk(x.re * p.re - x.im * p.im, x.re * p.im + x.im * p.re);
+                    for (int si = st.save_idx; si < d.nsave; si++)
+                        st2(d.save_out + (size_t)si * 2 * N, b, y);
+                    if (d.uL_out) st2(d.uL_out, b, y);
+                }
+                st.save_idx = d.nsave;
+                st.phase = d.mode == MODE_FORWARD ? PH_DONE : PH_SEED;
+            }
+            continue;
+        }
+
+        // PH_ADJ
+        {
+            C* ko = Sol::kp(d.ka, st.akperm, st.stage);
+#pragma unroll
+            for (int s = 0; s < E; s++) ko[Sol::bin(s)] = v[s];
+            if (st.stage < 6) {
+                st.stage++;
+                continue;
+            }
+            st.stage = 0;
+            const double z = st.cz, dt = st.cdt;
+            const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
+            const double EEst = S.error_norm(v, dt);
+            if (!isfinite(EEst)) {
+                st.status = ST_NONFINITE;
+                st.phase = PH_DONE;
+                continue;
+            }
+            double q11;
+            const double q = pi_q(EEst, st.aqold, q11);
+            st.a_nf += 6;
+            if (EEst > 1.0) {
+                st.a_nreject++;
+                st.adt = st.adt / fmin(1.0 / kQmin, q11 / kGamma);
+                continue;
+            }
+            st.a_naccept++;
+            double znew = z + dt;
+            if (fabs(znew - zlo) < 100.0 * kEps * fmax(z, zlo)) znew = zlo;
+            st.az = znew;
+            st.acur ^= 1;
+            st.akperm ^= 1;
+            st.aqold = fmax(EEst, kQoldInit);
+            const double adt = -dt;
+            st.adt = -fmin(fmax((q == 1.0) ? adt : adt / q, dtmin), L);
+            if (st.az == zlo) {
+                if (st.seg == 0) {
+                    st.phase = PH_FINAL;
+                } else {
+                    st.seg--;
+                    restore_checkpoint<R, LOGN, LOGE>(d, st.seg, st);
+                    st.phase = PH_REC;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0) states[slot] = st;
+}
+
+}  // namespace fl

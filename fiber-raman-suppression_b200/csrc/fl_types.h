@@ -1,0 +1,91 @@
+// fl_types.h -- slot descriptors and solver state shared by the host runtime
+// and the single-mode solver kernel.  Plain C layout (no CUDA types).
+#pragma once
+#include <stdint.h>
+
+namespace fl {
+
+enum SlotMode : int {
+    MODE_FORWARD = 0,        // forward only (propagate)
+    MODE_BAND_GRADIENT = 1,  // forward + Raman-band objective + adjoint + phase gradient
+    MODE_SEEDED_ADJOINT = 2  // forward + adjoint from a caller-supplied terminal seed
+};
+
+enum SlotPhase : int {
+    PH_FWD_INIT = 0,
+    PH_FWD = 1,
+    PH_SEED = 2,
+    PH_REC = 3,
+    PH_ADJ_INIT = 4,
+    PH_ADJ = 5,
+    PH_FINAL = 6,
+    PH_DONE = 7
+};
+
+// status codes (same values as the public FL_* codes)
+enum : int {
+    ST_OK = 0,
+    ST_NONFINITE = 2,
+    ST_DT_UNDERFLOW = 3,
+    ST_MAXITERS = 4,
+    ST_CAPACITY = 9
+};
+
+// Per-slot pointers and parameters.  R is float (FP32 mode) or double.
+// All field-sized buffers hold N complex values of the indicated type.
+template <typename R>
+struct SlotDesc {
+    // tables (shared by all slots of one fiber/grid)
+    const double* Dturns;   // D/(2 pi), turns per metre
+    const void* Heff;       // cx<R>: hR * (-1)^k  (fftshift folded in)
+    const void* ss;         // R: selfsteep = fftshift(ωs/ω0)
+    const void* tw;         // cx<R>: exp(-2 pi i k / N), k < N
+    double gamma, one_m_fR;
+    double L, reltol, abstol;
+    int mode, log_cost;
+    int nsave;
+    int ck_cap;             // checkpoint slots K (power of two)
+    int seg_cap;            // steps per recompute segment buffer
+    int step_cap;           // step-log capacity
+    long max_iters;         // attempted-step limit per integration
+    // caller data
+    const double* zsave;    // nsave save positions (sorted, first 0, last L)
+    double* save_out;       // nsave * N complex doubles, lab frame
+    const double* u0;       // N complex doubles: launch spectrum (shaped)
+    const unsigned char* mask;  // N band mask
+    const double* lamL;     // N complex doubles: caller terminal seed (lab frame)
+    double* lam0_out;       // N complex doubles (nullable)
+    double* grad_out;       // N doubles (nullable)
+    double* uL_out;         // N complex doubles: lab field at L (nullable)
+    // workspace
+    double* u[2];           // FP64 states
+    double* lam[2];         // FP64 adjoint states
+    void* kf[7];            // forward stages
+    void* ka[7];            // adjoint stages
+    void* scr[2];           // per-thread scratch fields
+    void* esv;              // error partial (cx<R>)
+    void* skv;              // error weights (R)
+    double* ck_u;           // ck_cap * N complex doubles
+    void* ck_k1;            // ck_cap * N cx<R>
+    double* steplog;        // 2 * step_cap doubles (z_n, dt_n)
+    void* seg;              // seg_cap * 5 * N cx<R>
+};
+
+struct SlotState {
+    int phase, status;
+    int cur, kperm;          // forward: u buffer index, FSAL permutation
+    int acur, akperm;        // adjoint: same
+    int nsteps, ck_stride, seg, save_idx;
+    int rec_pos;             // replayed steps within the current segment
+    int stage;               // stage of the attempt in progress (0 = none)
+    double cz, cdt;          // z and signed dt of the attempt in progress
+    double z, dt, qold;      // forward integrator
+    double az, adt, aqold;   // adjoint integrator
+    double abstol_adj;
+    double J;
+    long naccept, nreject, nf;
+    long a_naccept, a_nreject, a_nf;
+    long iters, a_iters;
+};
+
+}  // namespace fl

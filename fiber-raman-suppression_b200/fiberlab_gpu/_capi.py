@@ -1,0 +1,187 @@
+"""ctypes binding of the C-ABI declared in include/fiberlab_gpu.h.
+
+The shared library is built in-tree (fiberlab_gpu/libfiberlab_gpu.so).  There
+is no CPU fallback: loading fails loudly when the library is missing, and the
+calls fail with FL_ENODEV when no CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfiberlab_gpu.so")
+
+FL_OK = 0
+STATUS = {0: "FL_OK", 1: "FL_EINVAL", 2: "FL_NONFINITE", 3: "FL_DT_UNDERFLOW", 4: "FL_MAXITERS",
+          5: "FL_ENOMEM", 6: "FL_NONSYMMETRIC", 7: "FL_ENODEV", 8: "FL_ECUDA", 9: "FL_ECAPACITY",
+          10: "FL_EUNSUPPORTED", 11: "FL_OOM_ADMISSION", 12: "FL_EBUSY", 13: "FL_TIMEOUT"}
+PRECISION = {"fp32": 0, "fp64": 1}
+
+# every exported symbol of include/fiberlab_gpu.h (checked by the CPU tests)
+EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
+           "fl_last_error", "fl_ctx_launch_count", "fl_ctx_synchronize", "fl_problem_create",
+           "fl_problem_destroy", "fl_forward", "fl_adjoint", "fl_phase_gradient_batch",
+           "fl_phase_gradient_batch_device")
+
+
+class FlCtxOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("checkpoints", C.c_int),
+                ("segment_steps", C.c_int), ("step_log", C.c_int), ("max_iters", C.c_long)]
+
+
+class FlStats(C.Structure):
+    _fields_ = [("naccept", C.c_long), ("nreject", C.c_long), ("nf", C.c_long),
+                ("adj_naccept", C.c_long), ("adj_nreject", C.c_long), ("adj_nf", C.c_long),
+                ("status", C.c_int), ("checkpoints_used", C.c_int), ("J", C.c_double),
+                ("z_end", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class FiberLabGPUError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the CUDA library; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FiberLabGPUError(7, f"CUDA library not built: {LIB_PATH} is missing "
+                                      "(run __graft_entry__.build())")
+        lib = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.c_int, C.c_double
+        lib.fl_version.restype = C.c_char_p
+        lib.fl_status_string.restype = C.c_char_p
+        lib.fl_status_string.argtypes = [ip]
+        lib.fl_last_error.restype = C.c_char_p
+        lib.fl_last_error.argtypes = [vp]
+        lib.fl_ctx_create.argtypes = [ip, C.POINTER(FlCtxOpts), C.POINTER(vp)]
+        lib.fl_ctx_destroy.argtypes = [vp]
+        lib.fl_ctx_launch_count.restype = C.c_long
+        lib.fl_ctx_launch_count.argtypes = [vp]
+        lib.fl_ctx_synchronize.argtypes = [vp]
+        lib.fl_problem_create.argtypes = [vp, ip, ip, vp, vp, vp, vp, dp, dp, dp, dp, ip,
+                                          C.POINTER(vp)]
+        lib.fl_problem_destroy.argtypes = [vp]
+        lib.fl_forward.argtypes = [vp, vp, vp, ip, vp, C.POINTER(FlStats)]
+        lib.fl_adjoint.argtypes = [vp, vp, vp, C.POINTER(FlStats)]
+        lib.fl_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
+        lib.fl_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
+        _lib = lib
+    return _lib
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Context:
+    """fl_ctx on one device (one per host thread)."""
+
+    def __init__(self, device: int = 0, checkpoints: int = 32, segment_steps: int = 16,
+                 step_log: int = 16384, max_iters: int = 100000, hbm_budget_bytes: int = 0):
+        lib = load()
+        self.opts = FlCtxOpts(hbm_budget_bytes, checkpoints, segment_steps, step_log, max_iters)
+        h = C.c_void_p()
+        rc = lib.fl_ctx_create(device, C.byref(self.opts), C.byref(h))
+        if rc:
+            raise FiberLabGPUError(rc, lib.fl_status_string(rc).decode())
+        self.h = h
+
+    def check(self, rc: int):
+        if rc != FL_OK:
+            raise FiberLabGPUError(rc, load().fl_last_error(self.h).decode())
+
+    @property
+    def launches(self) -> int:
+        return load().fl_ctx_launch_count(self.h)
+
+    def synchronize(self):
+        self.check(load().fl_ctx_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().fl_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GPUProblem:
+    """fl_problem: device-resident tables of one resolved problem."""
+
+    def __init__(self, ctx: Context, fp, precision: str = "fp32"):
+        self.ctx, self.fp = ctx, fp
+        nt, M = fp.nt, fp.M
+        self._D = np.ascontiguousarray(fp.D, dtype=np.float64)
+        self._g = np.ascontiguousarray(fp.gamma_ref_order(), dtype=np.float64)
+        self._h = np.ascontiguousarray(fp.hR, dtype=np.complex128)
+        self._s = np.ascontiguousarray(fp.selfsteep, dtype=np.float64)
+        h = C.c_void_p()
+        ctx.check(load().fl_problem_create(ctx.h, nt, M, _ptr(self._D), _ptr(self._g),
+                                           _ptr(self._h), _ptr(self._s), float(fp.one_m_fR),
+                                           float(fp.L), float(fp.reltol), float(fp.abstol),
+                                           PRECISION[precision], C.byref(h)))
+        self.h = h
+
+    def forward(self, u0=None, saveat=None):
+        fp = self.fp
+        u0 = np.ascontiguousarray(fp.uw0 if u0 is None else u0, dtype=np.complex128)
+        z = np.ascontiguousarray([0.0, fp.L] if saveat is None else saveat, dtype=np.float64)
+        out = np.empty((len(z), fp.M, fp.nt), dtype=np.complex128)
+        st = FlStats()
+        self.ctx.check(load().fl_forward(self.h, _ptr(u0), _ptr(z), len(z), _ptr(out),
+                                         C.byref(st)))
+        return out, st.as_dict()
+
+    def adjoint(self, lambdaL):
+        lam = np.ascontiguousarray(lambdaL, dtype=np.complex128)
+        out = np.empty_like(lam)
+        st = FlStats()
+        self.ctx.check(load().fl_adjoint(self.h, _ptr(lam), _ptr(out), C.byref(st)))
+        return out, st.as_dict()
+
+    def phase_gradient_batch(self, phases, mask=None, u0=None, log_cost=False):
+        fp = self.fp
+        ph = np.ascontiguousarray(np.atleast_2d(phases), dtype=np.float64)
+        B = ph.shape[0]
+        u0 = np.ascontiguousarray(fp.uw0 if u0 is None else u0, dtype=np.complex128)
+        m = np.ascontiguousarray(fp.mask if mask is None else mask, dtype=np.uint8)
+        J = np.empty(B)
+        g = np.empty((B, fp.nt))
+        st = (FlStats * B)()
+        self.ctx.check(load().fl_phase_gradient_batch(self.h, _ptr(u0), B, _ptr(ph), _ptr(m),
+                                                      int(log_cost), _ptr(J), _ptr(g), st))
+        return J, g, [s.as_dict() for s in st]
+
+    def phase_gradient_batch_device(self, d_u0: int, B: int, d_phases: int, d_mask: int,
+                                    d_J: int, d_grad: int, log_cost=False, with_stats=True):
+        st = (FlStats * B)() if with_stats else None
+        self.ctx.check(load().fl_phase_gradient_batch_device(
+            self.h, d_u0, B, d_phases, d_mask, int(log_cost), d_J, d_grad, st))
+        return [s.as_dict() for s in st] if with_stats else None
+
+    def close(self):
+        if getattr(self, "h", None):
+            load().fl_problem_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

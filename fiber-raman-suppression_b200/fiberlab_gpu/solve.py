@@ -1,0 +1,185 @@
+"""Reference-shaped entry points over the CUDA stepper.
+
+Mirrors FiberLab's solver boundary with the same names, argument meaning and
+error behaviour:
+
+  solve_disp_mmf(uω0, fiber, sim)            src/simulation/simulate_disp_mmf.jl:183-207
+  solve_adjoint_disp_mmf(λωL, ũω, fiber, sim) src/simulation/sensitivity_disp_mmf.jl:309-332
+  propagate(problem; saveat)                 src/fiberlab/propagation.jl:89-123
+  physical phase gradient                    src/fiberlab/physics_models.jl:1033-1046
+
+`fiber` and `sim` are the reference's dictionaries (keys "Dω", "γ", "hRω",
+"one_m_fR", "L", "zsave", optional "reltol"/"abstol"; "Nt", "M", "ωs", "ω0",
+"Δt").  Fields are numpy arrays of shape (M, Nt) -- the memory layout of the
+reference's column-major (Nt, M) arrays.  Every solve runs on the GPU; there
+is no CPU path.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import problem as P
+from ._capi import Context, GPUProblem
+
+_DEFAULT_CTX: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _DEFAULT_CTX
+    if _DEFAULT_CTX is None:
+        _DEFAULT_CTX = Context(0)
+    return _DEFAULT_CTX
+
+
+def problem_from_dicts(uw0, fiber: dict, sim: dict) -> P.FiberProblem:
+    """The reference's (uω0, fiber, sim) triple as a FiberProblem
+    (required keys physics_models.jl:463-465)."""
+    for key in ("Nt", "M", "ωs", "ω0", "Δt"):
+        if key not in sim:
+            raise P.ArgumentError(f"sim is missing required key {key!r}")
+    for key in ("Dω", "γ", "hRω", "one_m_fR", "L"):
+        if key not in fiber:
+            raise P.ArgumentError(f"fiber is missing required key {key!r}")
+    gamma = np.asarray(fiber["γ"])
+    if not np.isrealobj(gamma):
+        raise P.ArgumentError("gamma tensor must use real-valued storage")
+    fp = P.FiberProblem(sim=sim, D=np.asarray(fiber["Dω"], dtype=np.float64),
+                        gamma=np.asarray(gamma, dtype=np.float64),
+                        hR=np.asarray(fiber["hRω"], dtype=np.complex128),
+                        one_m_fR=float(fiber["one_m_fR"]), L=float(fiber["L"]),
+                        uw0=np.asarray(uw0, dtype=np.complex128),
+                        reltol=float(fiber.get("reltol", 1e-8)),
+                        abstol=float(fiber.get("abstol", 1e-6)))
+    fp.validate()
+    return fp
+
+
+@dataclass
+class DEStats:
+    naccept: int
+    nreject: int
+    nf: int
+
+
+class GPUSolution:
+    """Stands in for the ODESolution of the reference solves: `sol(z)` at the
+    stored positions (interaction frame), `t`, `retcode`, `destats`.  The
+    forward keeps its z-checkpoints on the device for a following adjoint."""
+
+    def __init__(self, gp: GPUProblem, t, u, stats, frame="interaction", D=None):
+        self._gp = gp
+        self.t = np.asarray(t, dtype=np.float64)
+        self.u = u
+        self.retcode = "Success"
+        self.stats = stats
+        if frame == "adjoint":
+            self.destats = DEStats(stats["adj_naccept"], stats["adj_nreject"], stats["adj_nf"])
+        else:
+            self.destats = DEStats(stats["naccept"], stats["nreject"], stats["nf"])
+
+    def __call__(self, z: float):
+        idx = np.nonzero(self.t == z)[0]
+        if len(idx) == 0:
+            raise P.ArgumentError(
+                f"z={z} is not a stored position; pass it in saveat/zsave")
+        return self.u[idx[0]]
+
+
+def solve_disp_mmf(uw0, fiber: dict, sim: dict, *, precision="fp32", ctx: Context = None,
+                   saveat=None) -> dict:
+    """Forward solve 0 -> L (simulate_disp_mmf.jl:183-207).  Returns
+    {"ode_sol": GPUSolution} and, when fiber["zsave"] is set, the lab-frame
+    "uω_z" (Nz, M, Nt) and time-domain "ut_z" (fft along time)."""
+    fp = problem_from_dicts(uw0, fiber, sim)
+    ctx = ctx or default_context()
+    gp = GPUProblem(ctx, fp, precision)
+    zsave = fiber.get("zsave")
+    zs = [0.0, fp.L]
+    if zsave is not None:
+        zs = sorted(set([0.0, fp.L] + [float(z) for z in zsave]))
+    if saveat is not None:
+        zs = sorted(set(zs + [float(z) for z in saveat]))
+    lab, stats = gp.forward(fp.uw0, zs)
+    # interaction frame: ũ(z) = e^{-iDz} u(z)
+    inter = np.stack([np.exp(-1j * fp.D * z) * lab[i] for i, z in enumerate(zs)])
+    out = {"ode_sol": GPUSolution(gp, zs, inter, stats)}
+    if zsave is not None:
+        sel = [zs.index(float(z)) for z in zsave]
+        out["uω_z"] = lab[sel]
+        out["ut_z"] = np.fft.fft(lab[sel], axis=-1)
+    return out
+
+
+def solve_adjoint_disp_mmf(lamL, sol: GPUSolution, fiber: dict, sim: dict) -> GPUSolution:
+    """Adjoint solve L -> 0 (sensitivity_disp_mmf.jl:309-332); `sol(0)` is λ(0)."""
+    reltol = float(fiber.get("reltol", 1e-8))
+    abstol = float(fiber.get("abstol", 1e-6))
+    if not (np.isfinite(reltol) and reltol > 0):
+        raise P.ArgumentError("adjoint reltol must be positive and finite")
+    if not (np.isfinite(abstol) and abstol > 0):
+        raise P.ArgumentError("adjoint abstol must be positive and finite")
+    lam = np.asarray(lamL, dtype=np.complex128)
+    if not np.all(np.isfinite(lam)):
+        raise P.ArgumentError("adjoint terminal condition must be finite")
+    if not P.gamma_symmetric(np.asarray(fiber["γ"], dtype=np.float64)):
+        raise P.ArgumentError("fiber adjoint requires a fully permutation-symmetric gamma tensor")
+    lam0, stats = sol._gp.adjoint(lam)
+    L = float(fiber["L"])
+    return GPUSolution(sol._gp, [0.0, L], np.stack([lam0, np.exp(-1j * np.asarray(fiber["Dω"]) * L) * lam]),
+                       stats, frame="adjoint")
+
+
+@dataclass
+class PropagationResult:
+    """Lab-frame samples of one run (propagation.jl:5-23); spectra (Nz, M, Nt)."""
+    z_m: np.ndarray
+    spectra: np.ndarray
+    input_spectrum: np.ndarray
+    output_spectrum: np.ndarray
+    accepted_steps: int
+    rhs_evaluations: int
+
+
+def save_positions(saveat, length_m: float) -> np.ndarray:
+    """_save_positions (propagation.jl:60-70)."""
+    if saveat is None:
+        return np.array([0.0, length_m])
+    z = np.asarray(saveat, dtype=np.float64)
+    if z.ndim != 1:
+        raise P.ArgumentError("saveat must be a vector of distances")
+    if len(z) < 2:
+        raise P.ArgumentError("saveat must include 0 and the fiber length")
+    if not np.all(np.isfinite(z)):
+        raise P.ArgumentError("saveat distances must be finite")
+    if not np.all(np.diff(z) > 0):
+        raise P.ArgumentError("saveat distances must be sorted and unique")
+    if not (z[0] == 0.0 and z[-1] == length_m):
+        raise P.ArgumentError(f"saveat must start at 0 and end at the fiber length {length_m}")
+    return z
+
+
+def propagate(fp: P.FiberProblem, saveat=None, *, precision="fp32",
+              ctx: Context = None) -> PropagationResult:
+    """propagate(problem; saveat) (propagation.jl:89-123)."""
+    fp.validate()
+    z = save_positions(saveat, fp.L)
+    gp = GPUProblem(ctx or default_context(), fp, precision)
+    spectra, stats = gp.forward(fp.uw0, z)
+    return PropagationResult(z_m=z, spectra=spectra, input_spectrum=spectra[0].copy(),
+                             output_spectrum=spectra[-1].copy(),
+                             accepted_steps=stats["naccept"], rhs_evaluations=stats["nf"])
+
+
+def phase_gradient(fp: P.FiberProblem, phases, *, log_cost=False, precision="fp32",
+                   ctx: Context = None):
+    """Raman-band cost J and ∂J/∂φ for one or more vector phases
+    (physics_models.jl:1033-1046 with physics_helpers.jl:222-232)."""
+    if fp.mask is None or not np.any(fp.mask):
+        raise P.ArgumentError("band mask must contain at least one bin")
+    if not P.gamma_symmetric(fp.gamma):
+        raise P.ArgumentError("fiber adjoint requires a fully permutation-symmetric gamma tensor")
+    gp = GPUProblem(ctx or default_context(), fp, precision)
+    return gp.phase_gradient_batch(phases, fp.mask, fp.uw0, log_cost)

@@ -1,0 +1,147 @@
+/*
+ * fiberlab_gpu.h -- C-ABI of the B200 GMMNLSE stepper (forward propagation and
+ * adjoint gradient of FiberLab's interaction-picture solver).
+ *
+ * The reference has no FFI layer: its boundary is two Julia functions,
+ *   solve_disp_mmf(uω0, fiber, sim)            src/simulation/simulate_disp_mmf.jl:183
+ *   solve_adjoint_disp_mmf(λωL, ũω, fiber, sim) src/simulation/sensitivity_disp_mmf.jl:309
+ * and the callers built on them (propagate, src/fiberlab/propagation.jl:89;
+ * the adjoint model's physical gradient, src/fiberlab/physics_models.jl:1033-1046).
+ * Each entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *  - All functions return an int status (FL_OK = 0); no exception or longjmp
+ *    crosses the ABI.  fl_last_error(ctx) returns the message of the last
+ *    failure on that context.
+ *  - Arrays are the reference's column-major Julia arrays, passed as plain
+ *    host pointers: a field (Nt, M) of ComplexF64 is 2*Nt*M doubles with
+ *    element (t, i) at [2*(t + Nt*i)] (re) and [2*(t + Nt*i) + 1] (im);
+ *    D (Nt, M) is Nt*M doubles; gamma (M,M,M,M) is M^4 doubles with
+ *    γ[i,j,k,l] at i + M*(j + M*(k + M*l)).
+ *  - Host buffers are copied in and out; device buffers are owned by the
+ *    context/problem.  Functions with the _device suffix take device pointers
+ *    (already resident in HBM) instead.
+ *  - One context per host thread: calls on one context are not thread-safe.
+ *  - The GPU path is the only path: when no CUDA device or kernel image is
+ *    available the calls fail with FL_ENODEV; there is no CPU fallback.
+ */
+#ifndef FIBERLAB_GPU_H
+#define FIBERLAB_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (the solver codes mirror the reference's failure modes) */
+#define FL_OK 0
+#define FL_EINVAL 1          /* ArgumentError in the reference */
+#define FL_NONFINITE 2       /* NaN/Inf in a stage or result */
+#define FL_DT_UNDERFLOW 3    /* dt forced below floating-point resolution */
+#define FL_MAXITERS 4        /* attempted-step limit reached */
+#define FL_ENOMEM 5          /* device allocation failed */
+#define FL_NONSYMMETRIC 6    /* adjoint needs a permutation-symmetric gamma */
+#define FL_ENODEV 7          /* no usable CUDA device / kernel image */
+#define FL_ECUDA 8           /* other CUDA runtime error */
+#define FL_ECAPACITY 9       /* checkpoint/segment/step-log capacity exceeded */
+#define FL_EUNSUPPORTED 10   /* shape not built (e.g. Nt outside 2^6..2^14) */
+#define FL_OOM_ADMISSION 11  /* serving: request larger than the HBM budget */
+#define FL_EBUSY 12          /* serving: request not finished */
+#define FL_TIMEOUT 13        /* serving: wait limit reached */
+
+#define FL_PRECISION_FP32 0  /* FP32 bulk, FP64 phase/norm/reductions/state */
+#define FL_PRECISION_FP64 1  /* all arithmetic in FP64 */
+
+typedef struct fl_ctx fl_ctx;
+typedef struct fl_problem fl_problem;
+typedef struct fl_server fl_server;
+
+typedef struct {
+    size_t hbm_budget_bytes;   /* 0: no limit beyond cudaMalloc */
+    int checkpoints;           /* z-checkpoint slots K for the adjoint (power of 2, default 32) */
+    int segment_steps;         /* forward steps kept per recompute segment (default 16) */
+    int step_log;              /* accepted-step log capacity (default 16384) */
+    long max_iters;            /* attempted steps per integration (default 100000, as maxiters) */
+} fl_ctx_opts;
+
+/* Per-solve counters, mirroring destats.naccept/.nreject/.nf of the forward
+ * ODESolution (src/fiberlab/propagation.jl:105-108) and of the adjoint. */
+typedef struct {
+    long naccept, nreject, nf;
+    long adj_naccept, adj_nreject, adj_nf;
+    int status;
+    int checkpoints_used;
+    double J;          /* objective value (band gradient calls) */
+    double z_end;
+} fl_stats;
+
+/* Library version string and status names. */
+const char *fl_version(void);
+const char *fl_status_string(int status);
+
+/* Context on one CUDA device. */
+int fl_ctx_create(int device, const fl_ctx_opts *opts, fl_ctx **out);
+int fl_ctx_destroy(fl_ctx *ctx);
+const char *fl_last_error(const fl_ctx *ctx);
+/* Kernel launches issued by this context since creation (evidence counter). */
+long fl_ctx_launch_count(const fl_ctx *ctx);
+/* Synchronise the context's stream. */
+int fl_ctx_synchronize(fl_ctx *ctx);
+
+/* Upload one resolved problem: the tables get_p_disp_mmf builds from the
+ * `fiber`/`sim` dictionaries (simulate_disp_mmf.jl:87-114,
+ * sensitivity_disp_mmf.jl:237-283; required keys physics_models.jl:463-465).
+ *   D        (Nt, M) dispersion Dω [rad/m]
+ *   gamma    (M,M,M,M) real Kerr tensor [1/(W m)]
+ *   hR       Nt complex (interleaved) Raman spectrum hRω, Hermitian
+ *   selfsteep Nt: fftshift(ωs/ω0)
+ * Validation mirrors the reference: real finite gamma
+ * (simulate_disp_mmf.jl:62-67), Hermitian hR (physics_models.jl:438-449),
+ * positive finite L, reltol, abstol (propagation.jl:41-44). */
+int fl_problem_create(fl_ctx *ctx, int nt, int m, const double *D, const double *gamma,
+                      const double *hR, const double *selfsteep, double one_m_fR, double L,
+                      double reltol, double abstol, int precision, fl_problem **out);
+int fl_problem_destroy(fl_problem *prob);
+
+/* Forward solve 0 -> L.  Replaces solve_disp_mmf (simulate_disp_mmf.jl:183-207)
+ * as used by propagate (propagation.jl:89-123): out_spectra receives the
+ * lab-frame spectra cis(D z) ũ(z) at each saveat position (Nt*M*nsave
+ * complex, position-major; saveat sorted, first 0, last L, as
+ * propagation.jl:60-70 requires).  The forward state is kept (z-checkpoints)
+ * for a following fl_adjoint. */
+int fl_forward(fl_problem *prob, const double *u0, const double *saveat, int nsave,
+               double *out_spectra, fl_stats *stats);
+
+/* Adjoint solve L -> 0 from a lab-frame terminal seed λ(L), using the
+ * checkpoints of the last fl_forward on this problem (recomputing the
+ * forward field segment by segment).  Replaces solve_adjoint_disp_mmf
+ * (sensitivity_disp_mmf.jl:309-332): lambda0 receives sol(0).
+ * Fails with FL_NONSYMMETRIC for a gamma tensor that is not
+ * permutation-symmetric (sensitivity_disp_mmf.jl:103-112, 239-240). */
+int fl_adjoint(fl_problem *prob, const double *lambdaL, double *lambda0, fl_stats *stats);
+
+/* Batched forward + Raman-band objective + adjoint + spectral-phase gradient:
+ * the physical-gradient closure of spectral_shaper_model
+ * (physics_models.jl:1033-1046) with the band cost/seed of
+ * _field_spectral_band_cost (physics_helpers.jl:222-232, dB form :320-326),
+ * for nbatch independent launches u0 * cis(phases[:, b]).
+ *   u0      (Nt, M) launch spectrum
+ *   phases  (Nt, nbatch) vector phase per problem (shared across modes)
+ *   mask    Nt bytes, 1 in the band
+ *   J       nbatch objective values; grad (Nt, nbatch) ∂J/∂φ summed over
+ *           modes (physics_models.jl:732-737); stats nbatch (nullable). */
+int fl_phase_gradient_batch(fl_problem *prob, const double *u0, int nbatch,
+                            const double *phases, const unsigned char *mask, int log_cost,
+                            double *J, double *grad, fl_stats *stats);
+
+/* Same with every array already in device memory (HBM-resident timing). */
+int fl_phase_gradient_batch_device(fl_problem *prob, const double *d_u0, int nbatch,
+                                   const double *d_phases, const unsigned char *d_mask,
+                                   int log_cost, double *d_J, double *d_grad,
+                                   fl_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

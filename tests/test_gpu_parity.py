@@ -1,0 +1,178 @@
+"""GPU parity tests: the CUDA stepper through the C-ABI against the FP64
+oracle (field ≤ 1e-5 relative L2 in FP32 mode, ≤ 1e-10 in FP64 mode; Raman
+band fraction within 0.01 dB; gradients ≤ 1e-3 relative to the oracle
+adjoint and to central differences)."""
+import numpy as np
+import pytest
+
+from fiberlab_gpu import problem as P
+from fiberlab_gpu._capi import Context, FiberLabGPUError, GPUProblem
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL_FP32 = 1e-5
+FIELD_TOL_FP64 = 1e-10
+GRAD_TOL = 1e-3
+DB_TOL = 0.01
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def cfg0(nt=8192, T=10.0, **kw):
+    return P.single_mode_problem(nt=nt, time_window_ps=T, L=0.5, power_w=0.1,
+                                 rep_rate_hz=80e6, validate_grid=False, **kw)
+
+
+@pytest.mark.parametrize("nt,T", [(256, 3.0), (1024, 10.0), (2048, 10.0), (4096, 10.0)])
+def test_forward_matches_oracle(gpu_ctx, nt, T):
+    fp = P.single_mode_problem(nt=nt, time_window_ps=T, L=0.3, power_w=0.1,
+                               rep_rate_hz=80.5e6, validate_grid=False)
+    out, st = GPUProblem(gpu_ctx, fp).forward()
+    ref, rst, _ = O.forward(fp)
+    assert rel(out[-1], ref[-1]) < FIELD_TOL_FP32
+    assert st["status"] == 0 and st["z_end"] == fp.L
+    assert st["nf"] == 3 + 6 * (st["naccept"] + st["nreject"])
+
+
+def test_forward_config0_shape(gpu_ctx):
+    # Nt = 2^13 over 10 ps, SMF-28, 0.5 m, 0.1 W / 80 MHz, 185 fs sech²
+    fp = cfg0()
+    out, st = GPUProblem(gpu_ctx, fp).forward()
+    ref, rst, _ = O.forward(fp)
+    assert rel(out[-1], ref[-1]) < FIELD_TOL_FP32
+    Jg = P.band_cost_and_seed(out[-1], fp.mask)[0]
+    Jo = P.band_cost_and_seed(ref[-1], fp.mask)[0]
+    assert abs(10 * np.log10(Jg) - 10 * np.log10(Jo)) < DB_TOL
+    n0, n1 = P.photon_number(out[0], fp.sim), P.photon_number(out[-1], fp.sim)
+    assert abs(n1 / n0 - 1) < 1e-5
+
+
+def test_analytic_cw_kerr_gpu(gpu_ctx):
+    nt, L, pw, g = 64, 5.0, 2.0, 0.73
+    sim = P.get_disp_sim_params(1550e-9, 1, nt, 10.0, 2)
+    launch = np.fft.ifft(np.full((1, nt), np.sqrt(pw), complex), axis=1)
+    fp = P.FiberProblem(sim=sim, D=np.zeros((1, nt)), gamma=np.full((1, 1, 1, 1), g),
+                        hR=np.zeros(nt, complex), one_m_fR=1.0, L=L, uw0=launch,
+                        reltol=1e-10, abstol=1e-12)
+    expected = launch * np.exp(1j * g * pw * L)
+    out64, _ = GPUProblem(gpu_ctx, fp, "fp64").forward()
+    assert rel(out64[-1], expected) < 1e-8
+    out32, _ = GPUProblem(gpu_ctx, fp, "fp32").forward()
+    assert rel(out32[-1], expected) < 1e-5
+
+
+@pytest.mark.parametrize("nt,T", [(256, 3.0), (2048, 10.0)])
+def test_fp64_mode_matches_oracle(gpu_ctx, nt, T):
+    fp = P.single_mode_problem(nt=nt, time_window_ps=T, L=0.3, power_w=0.1,
+                               rep_rate_hz=80.5e6, validate_grid=False)
+    out, st = GPUProblem(gpu_ctx, fp, "fp64").forward()
+    ref, rst, _ = O.forward(fp)
+    assert rel(out[-1], ref[-1]) < FIELD_TOL_FP64
+    assert st["naccept"] == rst["naccept"]
+
+
+def test_saveat_dense_output(gpu_ctx):
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    zs = [0.0, 0.1, 0.2345, 0.4, 0.5]
+    out, _ = GPUProblem(gpu_ctx, fp).forward(saveat=zs)
+    ref, _, _ = O.forward(fp, zsave=zs)
+    for i in range(len(zs)):
+        assert rel(out[i], ref[i]) < FIELD_TOL_FP32
+
+
+def test_seeded_adjoint_matches_oracle(gpu_ctx):
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    gp = GPUProblem(gpu_ctx, fp)
+    out, _ = gp.forward()
+    ref, _, dense = O.forward(fp, keep_dense=True)
+    seed = ref[-1] * np.linspace(0.2, 1.8, fp.nt)[None, :]
+    lam0, st = gp.adjoint(seed)
+    lref, _ = O.adjoint(fp, dense, seed)
+    assert rel(lam0, lref) < GRAD_TOL
+    assert st["adj_naccept"] > 0
+    # a second adjoint from the same forward checkpoints
+    lam0b, _ = gp.adjoint(2.0 * seed)
+    assert rel(lam0b, 2.0 * lref) < GRAD_TOL
+
+
+@pytest.mark.parametrize("log_cost", [False, True])
+def test_band_gradient_config1(gpu_ctx, log_cost):
+    # config 1: Nt=2^13, φ ~ N(0, 0.5²) seed 0, Raman band < -13 THz, 32 checkpoints
+    fp = cfg0()
+    phi = 0.5 * np.random.default_rng(0).standard_normal(fp.nt)
+    J, g, st = GPUProblem(gpu_ctx, fp).phase_gradient_batch(phi[None, :], log_cost=log_cost)
+    Jo, go, _ = O.phase_gradient(fp, phi)
+    if log_cost:
+        assert abs(J[0] - 10 * np.log10(Jo)) < DB_TOL
+        go = go * 10 / (np.log(10) * Jo)
+    else:
+        assert abs(10 * np.log10(J[0]) - 10 * np.log10(Jo)) < DB_TOL
+    assert rel(g[0], go) < GRAD_TOL
+    assert st[0]["checkpoints_used"] <= 32
+
+
+def test_gradient_central_differences(gpu_ctx):
+    # gradient vs central FD (h = 1e-4) along random unit directions, with the
+    # FD costs from FP64 GPU forward solves
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6, raman_threshold_thz=-5.0)
+    rng = np.random.default_rng(3)
+    phi = 0.5 * rng.standard_normal(fp.nt)
+    J, g, _ = GPUProblem(gpu_ctx, fp).phase_gradient_batch(phi[None, :])
+    gp64 = GPUProblem(gpu_ctx, fp, "fp64")
+
+    def cost(ph):
+        out, _ = gp64.forward(fp.uw0 * np.exp(1j * ph)[None, :])
+        return P.band_cost_and_seed(out[-1], fp.mask)[0]
+    for _ in range(8):
+        d = rng.standard_normal(fp.nt)
+        d /= np.linalg.norm(d)
+        h = 1e-4
+        fd = (cost(phi + h * d) - cost(phi - h * d)) / (2 * h)
+        assert abs(fd - g[0] @ d) <= GRAD_TOL * abs(fd) + 1e-12
+
+
+def test_batch_results_equal_alone_and_in_mix(gpu_ctx):
+    fp = P.single_mode_problem(nt=2048, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    rng = np.random.default_rng(7)
+    phis = 0.5 * rng.standard_normal((12, fp.nt))
+    gp = GPUProblem(gpu_ctx, fp)
+    Jb, gb, _ = gp.phase_gradient_batch(phis)
+    for b in (0, 5, 11):
+        Ja, ga, _ = GPUProblem(gpu_ctx, fp).phase_gradient_batch(phis[b:b + 1])
+        assert Ja[0] == Jb[b]
+        assert np.array_equal(ga[0], gb[b])
+
+
+def test_status_codes_without_a_fault(gpu_ctx):
+    # host-side injections, no GPU fault: non-Hermitian hR is rejected at
+    # upload; a huge γ overflows the field -> FL_NONFINITE; a tiny iteration
+    # cap -> FL_MAXITERS; a tiny segment cap -> FL_ECAPACITY
+    fp = P.single_mode_problem(nt=256, time_window_ps=3.0, L=0.3, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    bad = P.FiberProblem(**{**fp.__dict__})
+    bad.hR = fp.hR.copy()
+    bad.hR[1] += 0.1j
+    with pytest.raises(FiberLabGPUError) as e:
+        GPUProblem(gpu_ctx, bad)
+    assert e.value.status == 1
+    huge = P.FiberProblem(**{**fp.__dict__})
+    huge.gamma = np.full((1, 1, 1, 1), 1e30)
+    with pytest.raises(FiberLabGPUError) as e:
+        GPUProblem(gpu_ctx, huge).forward()
+    assert e.value.status in (2, 3)
+    with pytest.raises(FiberLabGPUError) as e:
+        GPUProblem(Context(0, max_iters=3), fp).forward()
+    assert e.value.status == 4
+    long = P.single_mode_problem(nt=256, time_window_ps=3.0, L=3.0, power_w=0.3,
+                                 rep_rate_hz=80.5e6)
+    with pytest.raises(FiberLabGPUError) as e:
+        GPUProblem(Context(0, checkpoints=2, segment_steps=1), long).phase_gradient_batch(
+            np.zeros((1, long.nt)))
+    assert e.value.status == 9
