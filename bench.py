@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Headline benchmark: batched FP32 forward+adjoint band-gradient solves on B200.
+
+Workload (one "step"): B independent single-mode inverse-design problems of
+the Nt = 2^13 / 10 ps / SMF-28 / 0.5 m / 0.1 W / 185 fs sech² shape, each
+with its own launch phase φ_b ~ N(0, 0.5²) (seeded), run forward, Raman-band
+objective (< -13 THz), adjoint with z-checkpoints (32 slots) + recompute,
+and phase gradient, all on the GPU in one batched call.  Metric: fwd+adjoint
+solves/s (higher is better), whole job over all ranks.  The plain
+one-at-a-time path (the same solve, one problem per call) and its latency
+quantiles are reported beside it.
+
+Multi-GPU: replicas only (independent problems per rank, no collective on
+the data path; a barrier brackets the timed region and the time is the max
+over ranks).  `--impl reference` times the CPU reference arm: the FP64 C
+restatement of the reference solver on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "fiber-raman-suppression_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "fwd+adjoint solves/s"
+UNIT = "solves/s"
+NT, T_PS, L_M, P_W, REP = 8192, 10.0, 0.5, 0.1, 80e6
+BYTES_FWD_STEP = 336  # per point per attempted forward step (FP32 complex field passes)
+BYTES_ADJ_STEP = 384  # per point per attempted adjoint step
+
+
+def workload_problem():
+    from fiberlab_gpu import problem as P
+    return P.single_mode_problem(nt=NT, time_window_ps=T_PS, L=L_M, power_w=P_W,
+                                 rep_rate_hz=REP, raman_threshold_thz=-13.0,
+                                 validate_grid=False)
+
+
+def phases(rank: int, B: int, nt: int) -> np.ndarray:
+    rng = np.random.default_rng(1000 + rank)
+    return 0.5 * rng.standard_normal((B, nt))
+
+
+def config(B, world, extra=None):
+    c = {"workload": f"single-mode inverse-design batch: Nt=2^13 over 10 ps, SMF-28, L=0.5 m, "
+                     f"0.1 W/80 MHz 185 fs sech², phase N(0,0.5²), Raman band < -13 THz, "
+                     f"fwd+adjoint with 32 z-checkpoints",
+         "batch_per_gpu": B, "global_batch": B * world, "nt": NT, "modes": 1,
+         "precision": "FP32 bulk; FP64 phase/error norm/reductions/gradient",
+         "parallelism": f"replicas x{world}", "l2": "inputs and per-slot workspaces > L2 (126 MB)"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per stepper launch from the committed ncu summary, scaled to
+    the workload's batch by attempted steps (see profiles/)."""
+    p = os.path.join(ROOT, "profiles", "sm_advance_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_baseline(fp, nthreads: int, nprob: int):
+    from oracle import oracle as O
+    ph = phases(999, nprob, fp.nt)
+    t0 = time.perf_counter()
+    J, g, ns, failed = O.batch_phase_gradient(fp, ph, fp.mask, nthreads)
+    dt = time.perf_counter() - t0
+    return nprob / dt, dt
+
+
+def init_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args):
+    world, rank, local = init_dist()
+    if rank != 0:
+        return
+    fp = workload_problem()
+    cores = os.cpu_count() or 1
+    nprob = max(cores, 8)
+    for _ in range(args.warmup):
+        cpu_baseline(fp, cores, cores)
+    times, done = [], 0
+    for _ in range(args.steps):
+        _, dt = cpu_baseline(fp, cores, nprob)
+        times.append(dt)
+        done += nprob
+    value = done / sum(times)
+    sample = f"{nprob} problems per step (one per thread, {cores} threads)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(nprob, 1, {"implementation": "FP64 C restatement of the reference "
+                                        "Julia solver (Julia is not installed), OpenMP over "
+                                        "independent problems"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    world, rank, local = init_dist()
+    import torch
+    import torch.distributed as dist
+    from fiberlab_gpu._capi import Context, GPUProblem
+
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    ctx = Context(local, checkpoints=32, segment_steps=16)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    B = args.batch or 4 * sms
+    fp = workload_problem()
+    gp = GPUProblem(ctx, fp, "fp32")
+    ph_host = phases(rank, B, fp.nt)
+    d_u0 = torch.from_numpy(np.ascontiguousarray(fp.uw0).view(np.float64).copy()).to(dev)
+    d_ph = torch.from_numpy(ph_host).to(dev)
+    d_mask = torch.from_numpy(fp.mask.astype(np.uint8)).to(dev)
+    d_J = torch.empty(B, dtype=torch.float64, device=dev)
+    d_g = torch.empty((B, fp.nt), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        return gp.phase_gradient_batch_device(d_u0.data_ptr(), B, d_ph.data_ptr(),
+                                              d_mask.data_ptr(), d_J.data_ptr(), d_g.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    launches0 = ctx.launches
+    call_ms, kern_ms, stats_all = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()                      # L2 flush between timed iterations (not timed)
+        torch.cuda.synchronize(dev)
+        st = step()                        # synchronises the context stream
+        c, k = ctx.timing()
+        call_ms.append(c)
+        kern_ms.append(k)
+        stats_all.append(st)
+    torch.cuda.synchronize(dev)
+    launches = ctx.launches - launches0
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    t_rank = sum(call_ms)
+    if world > 1:
+        tt = torch.tensor([t_rank], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_job = float(tt.item())
+    else:
+        t_job = t_rank
+    value = B * args.steps * world / (t_job / 1e3)
+
+    # roofline of the stepper kernel: algorithmic bytes per launch / launch time
+    st = stats_all[-1]
+    fwd_att = sum(s["naccept"] + s["nreject"] for s in st)
+    rec = sum(s["naccept"] for s in st)
+    adj_att = sum(s["adj_naccept"] + s["adj_nreject"] for s in st)
+    alg_bytes = (BYTES_FWD_STEP * (fwd_att + rec) + BYTES_ADJ_STEP * adj_att) * fp.nt
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (kern_ms[-1] / 1e3) / 1e9
+    tr = profiled_traffic()
+    traffic = None
+    if tr and tr.get("bytes_per_attempted_step"):
+        traffic = tr["bytes_per_attempted_step"] * (fwd_att + rec + adj_att)
+
+    # end to end through the public host API (host buffers, copies inside)
+    e2e_t = []
+    for _ in range(max(2, min(args.steps, 3))):
+        t0 = time.perf_counter()
+        gp.phase_gradient_batch(ph_host, fp.mask, fp.uw0)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_value = B * world / max(np.mean(e2e_t), 1e-12)
+    h2d = ph_host.nbytes + fp.uw0.nbytes + fp.mask.nbytes
+    d2h = B * 8 + B * fp.nt * 8
+
+    # plain one-at-a-time drop-in (same solve, one problem per call)
+    plain_lat = []
+    for b in range(args.plain):
+        t0 = time.perf_counter()
+        gp.phase_gradient_batch(ph_host[b:b + 1], fp.mask, fp.uw0)
+        plain_lat.append(time.perf_counter() - t0)
+    plain = {"solves_per_s": 1.0 / float(np.mean(plain_lat)),
+             "latency_ms_p50": 1e3 * float(np.percentile(plain_lat, 50)),
+             "latency_ms_p99": 1e3 * float(np.percentile(plain_lat, 99))}
+    batched_lat = {"latency_ms_p50": float(np.percentile(call_ms, 50)),
+                   "latency_ms_p99": float(np.percentile(call_ms, 99))}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cores = os.cpu_count() or 1
+        v, dt = cpu_baseline(fp, cores, cores)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{cores} problems of this workload, one per thread ({dt:.1f} s)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": t_job / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config(B, world),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h)},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak,
+                             "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                             "peak_source": peak_kind,
+                             "kernel": "sm_advance_kernel<float,13,4>",
+                             "alg_bytes_per_launch": alg_bytes},
+                "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
+                "plain_one_at_a_time": plain, "batched": batched_lat,
+                "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=0, help="problems per GPU (default 4 x SMs)")
+    ap.add_argument("--plain", type=int, default=8, help="one-at-a-time solves timed")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -25,6 +25,8 @@ struct fl_ctx {
     fl_ctx_opts opts{};
     long launches = 0;
     int sm_count = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // call start/end, kernel start/end
+    double call_ms = 0.0, kernel_ms = 0.0;
 };
 
 namespace {
@@ -288,9 +290,14 @@ int launch_slots(fl_ctx* ctx, fl_problem* pr, Work* w, int nactive, int max_eval
 
 int run_to_completion(fl_problem* pr, Work* w) {
     fl_ctx* ctx = pr->ctx;
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
     int rc = launch_slots(ctx, pr, w, w->B, 0x7fffffff);
     if (rc) return rc;
+    CU(cudaEventRecord(ctx->ev[3], ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+    ctx->kernel_ms = ms;
     return FL_OK;
 }
 
@@ -446,13 +453,20 @@ int fl_ctx_create(int device, const fl_ctx_opts* opts, fl_ctx** out) {
         delete ctx;
         return FL_ECUDA;
     }
+    for (auto& e : ctx->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            fl_ctx_destroy(ctx);
+            return FL_ECUDA;
+        }
     *out = ctx;
     return FL_OK;
 }
 
 int fl_ctx_destroy(fl_ctx* ctx) {
     if (!ctx) return FL_EINVAL;
-    cudaStreamDestroy(ctx->stream);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return FL_OK;
 }
@@ -460,6 +474,13 @@ int fl_ctx_destroy(fl_ctx* ctx) {
 const char* fl_last_error(const fl_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 long fl_ctx_launch_count(const fl_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int fl_ctx_timing(const fl_ctx* ctx, double* last_call_ms, double* last_kernel_ms) {
+    if (!ctx) return FL_EINVAL;
+    if (last_call_ms) *last_call_ms = ctx->call_ms;
+    if (last_kernel_ms) *last_kernel_ms = ctx->kernel_ms;
+    return FL_OK;
+}
 
 int fl_ctx_synchronize(fl_ctx* ctx) {
     if (!ctx) return FL_EINVAL;
@@ -610,11 +631,43 @@ int fl_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats*
     return FL_OK;
 }
 
+int fl_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const double* u_fwd,
+                double* du_out) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!u_in || !du_out || (adjoint && !u_fwd) || !std::isfinite(z))
+        return set_err(ctx, FL_EINVAL, "invalid argument");
+    if (adjoint && !pr->gamma_sym)
+        return set_err(ctx, FL_NONSYMMETRIC,
+                       "fiber adjoint requires a fully permutation-symmetric gamma tensor");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    const int fp64 = pr->precision == FL_PRECISION_FP64;
+    RhsFn fn = rhs_launcher(fp64, ilog2i(pr->nt));
+    if (!fn) return set_err(ctx, FL_EUNSUPPORTED, "Nt = %d is not built", pr->nt);
+    Work* w = nullptr;
+    rc = new_work(pr, 1, 0, MODE_FORWARD, &w);
+    if (rc) return rc;
+    std::unique_ptr<Work> hold(w);
+    const size_t bytes = 16 * (size_t)pr->nt * pr->m;
+    CU(cudaMemcpyAsync(w->d_u0, u_in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (adjoint)
+        CU(cudaMemcpyAsync(w->d_lamL, u_fwd, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    RhsArgs a{w->d_desc, adjoint, z, w->d_u0, adjoint ? w->d_lamL : nullptr, w->d_lam0,
+              ctx->stream};
+    CU(fn(a));
+    ctx->launches++;
+    CU(cudaMemcpyAsync(du_out, w->d_lam0, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
 static int phase_gradient_core(fl_problem* pr, Work* w, int nbatch, const double* d_u0,
                                const double* d_phases, const unsigned char* d_mask,
                                int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
     fl_ctx* ctx = pr->ctx;
     const int nt = pr->nt;
+    CU(cudaEventRecord(ctx->ev[0], ctx->stream));
     int rc = set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost);
     if (rc) return rc;
     CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState) * nbatch, ctx->stream));
@@ -633,9 +686,13 @@ static int phase_gradient_core(fl_problem* pr, Work* w, int nbatch, const double
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(d_grad, w->d_grad, 8 * (size_t)nt * nbatch, cudaMemcpyDeviceToDevice,
                        ctx->stream));
+    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
     std::vector<SlotState> st;
     rc = read_states(ctx, w, st);
     if (rc) return rc;
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    ctx->call_ms = ms;
     if (stats)
         for (int b = 0; b < nbatch; b++) fill_stats(st[b], &stats[b]);
     return status_of_slots(ctx, st);

@@ -142,12 +142,12 @@ struct FftShape {
     static constexpr int NPASS = NFULL + (REM > 0 ? 1 : 0);
 };
 
-// One Stockham pass p of radix RP with stride NS (= product of the previous
+// One Stockham pass of radix RP with stride ns (the product of the previous
 // radices).  FIRST: inputs come from registers; LAST: outputs stay in
 // registers.  Between passes the data goes through the padded smem buffer.
-template <typename R, int LOGN, int LOGE, int RP, int NS, bool FIRST, bool LAST, bool INV>
+template <typename R, int LOGN, int LOGE, int RP, bool FIRST, bool LAST, bool INV>
 __device__ __forceinline__ void stockham_pass(cx<R> (&v)[1 << LOGE], cx<R>* __restrict__ sm,
-                                              const cx<R>* __restrict__ tw) {
+                                              const cx<R>* __restrict__ tw, const int ns) {
     using S = FftShape<LOGN, LOGE>;
     constexpr int E = S::E, T = S::T, N = S::N;
     constexpr int BPT = E / RP;  // butterflies per thread
@@ -157,46 +157,58 @@ __device__ __forceinline__ void stockham_pass(cx<R> (&v)[1 << LOGE], cx<R>* __re
         for (int s = 0; s < E; s++) v[s] = sm[pad(t + T * s)];
         __syncthreads();
     }
+    const int tws = N / (ns * RP);
 #pragma unroll
     for (int q = 0; q < BPT; q++) {
         const int j = t + T * q;
-        if constexpr (NS > 1) {
-            const int m = j & (NS - 1);
-            constexpr int TWS = N / (NS * RP);
+        const int m = j & (ns - 1);
+        if constexpr (!FIRST) {
 #pragma unroll
             for (int r = 1; r < RP; r++) {
-                cx<R> w = tw[m * r * TWS];
+                cx<R> w = tw[m * r * tws];
                 if (INV) w.im = -w.im;
                 v[q + BPT * r] = cmul(v[q + BPT * r], w);
             }
         }
         dft_inreg<RP, INV, BPT>(v, q);
         if constexpr (!LAST) {
-            const int base = (j / NS) * NS * RP + (j & (NS - 1));
+            const int base = (j - m) * RP + m;
 #pragma unroll
-            for (int r = 0; r < RP; r++) sm[pad(base + r * NS)] = v[q + BPT * r];
+            for (int r = 0; r < RP; r++) sm[pad(base + r * ns)] = v[q + BPT * r];
         }
     }
     if constexpr (!LAST) __syncthreads();
 }
 
-template <typename R, int LOGN, int LOGE, bool INV, int P>
-__device__ __forceinline__ void fft_passes(cx<R> (&v)[1 << LOGE], cx<R>* sm, const cx<R>* tw) {
+// Block-wide unnormalised transform of the N values held in v (all threads
+// of the block must call it).  The passes between the first and the last
+// run as a runtime loop over one code body, so the whole kernel carries one
+// copy of each pass type.  The smem buffer must hold padded_len(N) elements.
+template <typename R, int LOGN, int LOGE, bool INV = false>
+__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], cx<R>* sm, const cx<R>* tw) {
     using S = FftShape<LOGN, LOGE>;
-    if constexpr (P < S::NPASS) {
-        constexpr int RP = (P < S::NFULL) ? S::E : (1 << S::REM);
-        constexpr int NS = 1 << (LOGE * P);
-        stockham_pass<R, LOGN, LOGE, RP, NS, P == 0, P == S::NPASS - 1, INV>(v, sm, tw);
-        fft_passes<R, LOGN, LOGE, INV, P + 1>(v, sm, tw);
+    constexpr int E = S::E;
+    constexpr int RL = S::REM ? (1 << S::REM) : E;  // radix of the last pass
+    if constexpr (S::NPASS == 1) {
+        dft_inreg<E, INV, 1>(v, 0);
+    } else {
+        stockham_pass<R, LOGN, LOGE, E, true, false, INV>(v, sm, tw, 1);
+        int ns = E;
+#pragma unroll 1
+        for (int p = 1; p < S::NPASS - 1; p++) {
+            stockham_pass<R, LOGN, LOGE, E, false, false, INV>(v, sm, tw, ns);
+            ns *= E;
+        }
+        stockham_pass<R, LOGN, LOGE, RL, false, true, INV>(v, sm, tw, ns);
     }
 }
 
-// Block-wide unnormalised transform of the N values held in v (all threads
-// of the block must call it).  The smem buffer must hold padded_len(N)
-// elements and must not be in use by the caller across this call.
-template <typename R, int LOGN, int LOGE, bool INV>
-__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], cx<R>* sm, const cx<R>* tw) {
-    fft_passes<R, LOGN, LOGE, INV, 0>(v, sm, tw);
+// unnormalised inverse (exponent sign +1) through the forward code path:
+// F⁻¹(x)·N = conj(F(conj(x)))
+template <typename R, int E>
+__device__ __forceinline__ void conj_all(cx<R> (&v)[E]) {
+#pragma unroll
+    for (int s = 0; s < E; s++) v[s].im = -v[s].im;
 }
 
 }  // namespace fl

@@ -18,6 +18,18 @@ struct LaunchArgs {
 
 using LaunchFn = cudaError_t (*)(const LaunchArgs&);
 
+struct RhsArgs {
+    const void* desc;      // one SlotDesc<R> (tables and scratch)
+    int adjoint;
+    double z;
+    const double* in;      // N complex doubles: ũ or λ̃
+    const double* ufwd;    // N complex doubles: forward field (adjoint)
+    double* out;           // N complex doubles
+    cudaStream_t stream;
+};
+using RhsFn = cudaError_t (*)(const RhsArgs&);
+RhsFn rhs_launcher(int fp64, int logn);
+
 // returns nullptr when (precision, log2 Nt) is not built
 LaunchFn sm_launcher(int fp64, int logn);
 // threads per CTA of a built launcher (0 when not built)

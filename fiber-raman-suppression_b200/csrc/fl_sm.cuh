@@ -144,96 +144,108 @@ struct SmSolver {
 
     __device__ __forceinline__ static int bin(int s) { return threadIdx.x + T * s; }
 
-    // forward RHS: v holds the stage input ũ (own bins) and receives dũ/dz
-    __device__ void rhs_fwd(double z, C (&v)[E]) {
+    // One right-hand-side evaluation, forward (adj = false) or adjoint, as a
+    // runtime loop over its transforms so the kernel holds one copy of the
+    // FFT code (inverse transforms run as conj∘F∘conj):
+    //   forward  f0: ũ e^{iDz} -F-> u_t       f1: (γ|u_t|², 0) -F->
+    //            f2: ·Heff -F⁻¹-> N h∗I       f3: ((1-fR)I + h∗I) u_t -F⁻¹->
+    //            post: dũ = i e^{-iDz} τ (·)/N
+    //   adjoint  f0: λ̃ e^{iDz} τ -F-> λ_t     f1: ũ(z) e^{iDz} -F-> u_t
+    //            f2: (I, Y) -F-> X            f3: split X into Î, Ŷ;
+    //                Heff Î + i conj(Heff) Ŷ -F⁻¹-> N (h∗I + i h̃⋆Y)
+    //            f4: η -F⁻¹->                post: dλ̃ = i e^{-iDz} (·)/N
+    // load_u(v) fills v with the forward field ũ(z) for the adjoint.
+    template <class LoadU>
+    __device__ void rhs(const bool adj, const double z, C (&v)[E], LoadU&& load_u) {
         const R g = (R)d.gamma, ofr = (R)d.one_m_fR, invn = R(1) / R(N);
+        const int nfft = adj ? 5 : 4;
+#pragma unroll 1
+        for (int f = 0; f < nfft; f++) {
+            bool inv = false;
+            const int op = adj ? 8 + f : f;
+            if (op == 0) {
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
-        block_fft<R, LOGN, LOGE, false>(v, sm, tw);
+                for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
+            } else if (op == 1) {
 #pragma unroll
-        for (int s = 0; s < E; s++) {
-            scr0[bin(s)] = v[s];
-            v[s] = mk(g * abs2(v[s]), R(0));
+                for (int s = 0; s < E; s++) {
+                    scr0[bin(s)] = v[s];
+                    v[s] = mk(g * abs2(v[s]), R(0));
+                }
+            } else if (op == 2) {
+#pragma unroll
+                for (int s = 0; s < E; s++) v[s] = cmul(v[s], Heff[bin(s)]);
+                inv = true;
+            } else if (op == 3) {
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const C ut = scr0[bin(s)];
+                    const R fac = ofr * (g * abs2(ut)) + v[s].re * invn;
+                    v[s] = scale(ut, fac);
+                }
+                inv = true;
+            } else if (op == 8) {
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = bin(s);
+                    v[s] = scale(cmul(v[s], phasor<R>(d.Dturns[b], z)), ss[b]);
+                }
+            } else if (op == 9) {
+#pragma unroll
+                for (int s = 0; s < E; s++) scr0[bin(s)] = v[s];
+                load_u(v);
+#pragma unroll
+                for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
+            } else if (op == 10) {
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = bin(s);
+                    const C lt = scr0[b];
+                    scr1[b] = v[s];
+                    const R I = g * abs2(v[s]);
+                    const R Y = g * (lt.im * v[s].re - lt.re * v[s].im);  // γ Im(λ u*)
+                    v[s] = mk(I, Y);
+                }
+            } else if (op == 11) {
+                // split the two real spectra with X[k] and conj(X[-k])
+#pragma unroll
+                for (int s = 0; s < E; s++) sm[pad(bin(s))] = v[s];
+                __syncthreads();
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = bin(s);
+                    const C zm = conjc(sm[pad((N - b) & (N - 1))]);
+                    const C H = Heff[b];
+                    const C a = scale(v[s] + zm, R(0.5));   // spectrum of I
+                    const C c = scale(v[s] - zm, R(0.5));   // i * spectrum of Y
+                    v[s] = cmul(a, H) + cmulc(c, H);
+                }
+                __syncthreads();
+                inv = true;
+            } else {  // op == 12
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int b = bin(s);
+                    const C lt = scr0[b], ut = scr1[b];
+                    const R I = g * abs2(ut);
+                    const R Rr = v[s].re * invn, Ri = v[s].im * invn;
+                    const C t1 = scale(lt, R(2) * ofr * I + Rr);
+                    const C t2 = scale(cmulc(cmul(ut, ut), lt), ofr * g);  // (1-fR)γ λ* u²
+                    const C t3 = mk(-R(2) * Ri * ut.im, R(2) * Ri * ut.re);  // 2i Ri u
+                    v[s] = t1 - t2 + t3;
+                }
+                inv = true;
+            }
+            if (inv) conj_all(v);
+            block_fft<R, LOGN, LOGE>(v, sm, tw);
+            if (inv) conj_all(v);
         }
-        block_fft<R, LOGN, LOGE, false>(v, sm, tw);
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = cmul(v[s], Heff[bin(s)]);
-        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const C ut = scr0[bin(s)];
-            const R f = ofr * (g * abs2(ut)) + v[s].re * invn;
-            v[s] = scale(ut, f);
-        }
-        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int b = bin(s);
             const C y = cmulc(v[s], phasor<R>(d.Dturns[b], z));  // e^{-iDz} x
-            const R sc = ss[b] * invn;
-            v[s] = mk(-y.im * sc, y.re * sc);                      // i * y * τ / N
-        }
-    }
-
-    // adjoint RHS: v holds the stage input λ̃ and receives dλ̃/dz; load_u(v)
-    // fills v with the forward field ũ(z) (one register array at a time)
-    template <class LoadU>
-    __device__ void rhs_adj(double z, C (&v)[E], LoadU&& load_u) {
-        const R g = (R)d.gamma, ofr = (R)d.one_m_fR, invn = R(1) / R(N);
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            v[s] = scale(cmul(v[s], phasor<R>(d.Dturns[b], z)), ss[b]);
-        }
-        block_fft<R, LOGN, LOGE, false>(v, sm, tw);   // λ_t
-#pragma unroll
-        for (int s = 0; s < E; s++) scr0[bin(s)] = v[s];
-        load_u(v);
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
-        block_fft<R, LOGN, LOGE, false>(v, sm, tw);   // u_t
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            const C lt = scr0[b];
-            scr1[b] = v[s];
-            const R I = g * abs2(v[s]);
-            const R Y = g * (lt.im * v[s].re - lt.re * v[s].im);  // γ Im(λ u*)
-            v[s] = mk(I, Y);
-        }
-        block_fft<R, LOGN, LOGE, false>(v, sm, tw);
-        // split the two real spectra: X[k] and conj(X[-k])
-#pragma unroll
-        for (int s = 0; s < E; s++) sm[pad(bin(s))] = v[s];
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            const C zm = conjc(sm[pad((N - b) & (N - 1))]);
-            const C H = Heff[b];
-            const C a = scale(v[s] + zm, R(0.5));   // spectrum of I
-            const C c = scale(v[s] - zm, R(0.5));   // i * spectrum of Y
-            v[s] = cmul(a, H) + cmulc(c, H);
-        }
-        __syncthreads();
-        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            const C lt = scr0[b], ut = scr1[b];
-            const R I = g * abs2(ut);
-            const R Rr = v[s].re * invn, Ri = v[s].im * invn;
-            const C t1 = scale(lt, R(2) * ofr * I + Rr);
-            const C u2 = cmul(ut, ut);
-            const C t2 = scale(cmulc(u2, lt), ofr * g);      // (1-fR) γ conj(λ) u²
-            const C t3 = mk(-R(2) * Ri * ut.im, R(2) * Ri * ut.re);  // 2i Ri u
-            v[s] = t1 - t2 + t3;
-        }
-        block_fft<R, LOGN, LOGE, true>(v, sm, tw);
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const C y = cmulc(v[s], phasor<R>(d.Dturns[bin(s)], z));
-            v[s] = mk(-y.im * invn, y.re * invn);
+            const R sc = adj ? invn : ss[b] * invn;
+            v[s] = mk(-y.im * sc, y.re * sc);                      // i y (τ) / N
         }
     }
 
@@ -364,7 +376,13 @@ struct SegLoader {
     Sol& S;
     int seg_lo, seg_hi;
     double zz;
+    const double* direct;  // FP64 field given directly (single RHS evaluations)
     __device__ void operator()(cx<R> (&w)[Sol::E]) const {
+        if (direct) {
+#pragma unroll
+            for (int s = 0; s < Sol::E; s++) w[s] = down<R>(ld2(direct, Sol::bin(s)));
+            return;
+        }
         const double* lg = S.d.steplog;
         int n = seg_lo;
         while (n + 1 < seg_hi && lg[2 * (n + 1)] <= zz) n++;
@@ -372,6 +390,62 @@ struct SegLoader {
         S.interp(n - seg_lo, dtn, (zz - zn) / dtn, w);
     }
 };
+
+// Out-of-line RHS evaluations.  The FFT-heavy bodies get the full register
+// budget of the CTA instead of sharing it with the state machine's live
+// values; the 2E-register field crosses the call through local memory.
+template <typename R, int LOGN, int LOGE>
+__device__ __noinline__ void rhs_fwd_call(const SlotDesc<R>* d, cx<R>* sm, double* red, double z,
+                                          cx<R>* vio) {
+    using Sol = SmSolver<R, LOGN, LOGE>;
+    Sol S(*d, sm, red);
+    cx<R> v[Sol::E];
+#pragma unroll
+    for (int s = 0; s < Sol::E; s++) v[s] = vio[s];
+    S.rhs(false, z, v, [](cx<R>(&)[Sol::E]) {});
+#pragma unroll
+    for (int s = 0; s < Sol::E; s++) vio[s] = v[s];
+}
+
+// ufwd != nullptr: the forward field is read from that FP64 buffer (single
+// RHS evaluations); otherwise from the dense interpolant of the segment
+template <typename R, int LOGN, int LOGE>
+__device__ __noinline__ void rhs_adj_call(const SlotDesc<R>* d, cx<R>* sm, double* red, double z,
+                                          cx<R>* vio, int seg_lo, int seg_hi, double zload,
+                                          const double* ufwd) {
+    using Sol = SmSolver<R, LOGN, LOGE>;
+    Sol S(*d, sm, red);
+    cx<R> v[Sol::E];
+#pragma unroll
+    for (int s = 0; s < Sol::E; s++) v[s] = vio[s];
+    SegLoader<R, LOGN, LOGE> ld{S, seg_lo, seg_hi, zload, ufwd};
+    S.rhs(true, z, v, ld);
+#pragma unroll
+    for (int s = 0; s < Sol::E; s++) vio[s] = v[s];
+}
+
+// One RHS evaluation on one CTA (unit parity of the right-hand sides):
+// in/ufwd/out are N complex doubles.
+template <typename R, int LOGN, int LOGE>
+__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+    sm_rhs_kernel(const SlotDesc<R>* __restrict__ d, int adjoint, double z,
+                  const double* __restrict__ in, const double* __restrict__ ufwd,
+                  double* __restrict__ out) {
+    using Sol = SmSolver<R, LOGN, LOGE>;
+    using C = cx<R>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    double* red = reinterpret_cast<double*>(smraw + sizeof(C) * padded_len(Sol::N));
+    C v[Sol::E];
+#pragma unroll
+    for (int s = 0; s < Sol::E; s++) v[s] = down<R>(ld2(in, Sol::bin(s)));
+    if (adjoint)
+        rhs_adj_call<R, LOGN, LOGE>(d, sm, red, z, v, 0, 0, 0.0, ufwd);
+    else
+        rhs_fwd_call<R, LOGN, LOGE>(d, sm, red, z, v);
+#pragma unroll
+    for (int s = 0; s < Sol::E; s++) st2(out, Sol::bin(s), up(v[s]));
+}
 
 template <typename R, int LOGN, int LOGE>
 __device__ __forceinline__ void restore_checkpoint(const SlotDesc<R>& d, int seg, SlotState& st) {
@@ -575,9 +649,17 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     st.phase = PH_DONE;
                     continue;
                 }
-                double adt = fmax(fmin(fabs(st.adt), L), dtmin);
+                // Segment starts are stopping points of this implementation only
+                // (the reference integrates the adjoint without them), so they
+                // are made transparent to the controller: no sliver step before
+                // one (the last two steps are split evenly) and the proposal
+                // from before the clip is restored after it.
+                const double prop = fmax(fmin(fabs(st.adt), L), dtmin);
                 const double rem = st.az - zlo;
-                if (adt > rem) adt = rem;
+                double adt = prop;
+                if (adt >= rem) adt = rem;
+                else if (adt > 0.5 * rem) adt = 0.5 * rem;
+                st.aprop = prop;
                 st.cz = st.az;
                 st.cdt = -adt;
                 st.stage = 1;
@@ -595,10 +677,9 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         if (adj) {
             const int seg_lo = st.seg * st.ck_stride;
             const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
-            SegLoader<R, LOGN, LOGE> ld{S, seg_lo, seg_hi, zload};
-            S.rhs_adj(ze, v, ld);
+            rhs_adj_call<R, LOGN, LOGE>(&d, sm, red, ze, v, seg_lo, seg_hi, zload, nullptr);
         } else {
-            S.rhs_fwd(ze, v);
+            rhs_fwd_call<R, LOGN, LOGE>(&d, sm, red, ze, v);
         }
         evals++;
 
@@ -867,7 +948,9 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             st.akperm ^= 1;
             st.aqold = fmax(EEst, kQoldInit);
             const double adt = -dt;
-            st.adt = -fmin(fmax((q == 1.0) ? adt : adt / q, dtmin), L);
+            double dtn = fmin(fmax((q == 1.0) ? adt : adt / q, dtmin), L);
+            if (adt < st.aprop) dtn = fmax(dtn, st.aprop);  // shortened for a segment start
+            st.adt = -dtn;
             if (st.az == zlo) {
                 if (st.seg == 0) {
                     st.phase = PH_FINAL;

@@ -79,6 +79,7 @@ struct SlotState {
     int rec_pos;             // replayed steps within the current segment
     int stage;               // stage of the attempt in progress (0 = none)
     double cz, cdt;          // z and signed dt of the attempt in progress
+    double aprop;            // adjoint: controller proposal before a segment clip
     double z, dt, qold;      // forward integrator
     double az, adt, aqold;   // adjoint integrator
     double abstol_adj;

@@ -24,7 +24,7 @@ PRECISION = {"fp32": 0, "fp64": 1}
 EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_last_error", "fl_ctx_launch_count", "fl_ctx_synchronize", "fl_problem_create",
            "fl_problem_destroy", "fl_forward", "fl_adjoint", "fl_phase_gradient_batch",
-           "fl_phase_gradient_batch_device")
+           "fl_phase_gradient_batch_device", "fl_rhs_eval", "fl_ctx_timing")
 
 
 class FlCtxOpts(C.Structure):
@@ -77,6 +77,8 @@ def load() -> C.CDLL:
         lib.fl_adjoint.argtypes = [vp, vp, vp, C.POINTER(FlStats)]
         lib.fl_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
+        lib.fl_rhs_eval.argtypes = [vp, ip, dp, vp, vp, vp]
+        lib.fl_ctx_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         _lib = lib
     return _lib
 
@@ -105,6 +107,12 @@ class Context:
     @property
     def launches(self) -> int:
         return load().fl_ctx_launch_count(self.h)
+
+    def timing(self):
+        """(last call ms, last stepper-kernel ms), CUDA events on the context stream."""
+        a, b = C.c_double(), C.c_double()
+        self.check(load().fl_ctx_timing(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def synchronize(self):
         self.check(load().fl_ctx_synchronize(self.h))
@@ -154,6 +162,15 @@ class GPUProblem:
         st = FlStats()
         self.ctx.check(load().fl_adjoint(self.h, _ptr(lam), _ptr(out), C.byref(st)))
         return out, st.as_dict()
+
+    def rhs(self, z, u, ufwd=None):
+        """One forward (ufwd None) or adjoint RHS evaluation on the GPU."""
+        u = np.ascontiguousarray(u, dtype=np.complex128)
+        out = np.empty_like(u)
+        uf = None if ufwd is None else np.ascontiguousarray(ufwd, dtype=np.complex128)
+        self.ctx.check(load().fl_rhs_eval(self.h, int(uf is not None), float(z), _ptr(u),
+                                          None if uf is None else _ptr(uf), _ptr(out)))
+        return out
 
     def phase_gradient_batch(self, phases, mask=None, u0=None, log_cost=False):
         fp = self.fp

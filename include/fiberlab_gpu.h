@@ -86,6 +86,10 @@ int fl_ctx_destroy(fl_ctx *ctx);
 const char *fl_last_error(const fl_ctx *ctx);
 /* Kernel launches issued by this context since creation (evidence counter). */
 long fl_ctx_launch_count(const fl_ctx *ctx);
+/* Device time of the last public call on this context, measured with CUDA
+ * events recorded on the context's stream: the whole call's GPU work and the
+ * stepper kernel launches alone (milliseconds). */
+int fl_ctx_timing(const fl_ctx *ctx, double *last_call_ms, double *last_kernel_ms);
 /* Synchronise the context's stream. */
 int fl_ctx_synchronize(fl_ctx *ctx);
 
@@ -134,6 +138,14 @@ int fl_adjoint(fl_problem *prob, const double *lambdaL, double *lambda0, fl_stat
 int fl_phase_gradient_batch(fl_problem *prob, const double *u0, int nbatch,
                             const double *phases, const unsigned char *mask, int log_cost,
                             double *J, double *grad, fl_stats *stats);
+
+/* One evaluation of the forward right-hand side disp_mmf!
+ * (simulate_disp_mmf.jl:25-60) or, with adjoint = 1, of adjoint_disp_mmf!
+ * (sensitivity_disp_mmf.jl:32-79) with the forward field u_fwd given
+ * directly instead of through the interpolant.  u_in, u_fwd, du_out are
+ * (Nt, M) complex host arrays in the interaction picture at position z. */
+int fl_rhs_eval(fl_problem *prob, int adjoint, double z, const double *u_in,
+                const double *u_fwd, double *du_out);
 
 /* Same with every array already in device memory (HBM-resident timing). */
 int fl_phase_gradient_batch_device(fl_problem *prob, const double *d_u0, int nbatch,

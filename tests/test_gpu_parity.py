@@ -26,6 +26,23 @@ def cfg0(nt=8192, T=10.0, **kw):
                                  rep_rate_hz=80e6, validate_grid=False, **kw)
 
 
+@pytest.mark.parametrize("nt", [64, 256, 1024, 8192, 16384])
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_rhs_matches_oracle(gpu_ctx, nt, precision):
+    if precision == "fp64" and nt > 8192:
+        pytest.skip("FP64 mode is built up to 2^13")
+    fp = P.single_mode_problem(nt=nt, time_window_ps=10.0 if nt >= 1024 else 3.0, L=0.5,
+                               power_w=0.1, rep_rate_hz=80.5e6, validate_grid=False)
+    rng = np.random.default_rng(nt)
+    u = fp.uw0 * np.exp(0.3j * rng.standard_normal(fp.nt))[None, :]
+    lam = (rng.standard_normal(fp.nt) + 1j * rng.standard_normal(fp.nt))[None, :] * 1e-3
+    gp = GPUProblem(gpu_ctx, fp, precision)
+    z = 0.3217
+    tol = 2e-6 if precision == "fp32" else 1e-12
+    assert rel(gp.rhs(z, u), O.rhs_forward(fp, z, u)) < tol
+    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < tol
+
+
 @pytest.mark.parametrize("nt,T", [(256, 3.0), (1024, 10.0), (2048, 10.0), (4096, 10.0)])
 def test_forward_matches_oracle(gpu_ctx, nt, T):
     fp = P.single_mode_problem(nt=nt, time_window_ps=T, L=0.3, power_w=0.1,
@@ -60,6 +77,8 @@ def test_analytic_cw_kerr_gpu(gpu_ctx):
     expected = launch * np.exp(1j * g * pw * L)
     out64, _ = GPUProblem(gpu_ctx, fp, "fp64").forward()
     assert rel(out64[-1], expected) < 1e-8
+    # FP32 mode at the default tolerances (FP32 cannot meet abstol 1e-12)
+    fp.reltol, fp.abstol = 1e-8, 1e-6
     out32, _ = GPUProblem(gpu_ctx, fp, "fp32").forward()
     assert rel(out32[-1], expected) < 1e-5
 
