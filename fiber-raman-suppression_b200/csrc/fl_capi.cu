@@ -127,9 +127,9 @@ struct fl_problem {
     double one_m_fR = 0, L = 0, reltol = 0, abstol = 0, gamma0 = 0;
     bool gamma_sym = true;
     double* d_Dturns = nullptr;
-    void* d_Heff = nullptr;
-    void* d_ss = nullptr;
-    void* d_tw = nullptr;
+    void* d_Heff[2] = {nullptr, nullptr};  // [0] float, [1] double
+    void* d_ss[2] = {nullptr, nullptr};
+    void* d_tw[2] = {nullptr, nullptr};
     // workspace of the last forward (kept for fl_adjoint)
     struct Work* last = nullptr;
 };
@@ -140,7 +140,7 @@ struct Work {
     int B = 0, nt = 0, rsize = 4, K = 0, segcap = 0, stepcap = 0, nsave = 0;
     char* pool = nullptr;
     size_t pool_bytes = 0;
-    void* d_desc = nullptr;          // SlotDesc<R>[B]
+    void* d_desc = nullptr;          // SlotDesc[B]
     SlotState* d_state = nullptr;    // [B]
     int* d_active = nullptr;         // [B]
     std::vector<unsigned char> h_desc;  // host image of the descriptors
@@ -163,13 +163,13 @@ struct Work {
 
 namespace {
 
-template <typename R>
-size_t slot_bytes(int nt, int K, int segcap, int stepcap) {
-    const size_t C = 2 * sizeof(R) * nt, D2 = 16 * (size_t)nt;
+// rf: bytes of one forward-precision real (4 or 8); the adjoint is FP64
+size_t slot_bytes(int nt, size_t rf, int K, int segcap, int stepcap) {
+    const size_t C = 2 * rf * nt, D2 = 16 * (size_t)nt;
     size_t b = 0;
     b += 2 * D2 + 2 * D2;               // u[2], lam[2]
-    b += 14 * C;                        // kf, ka
-    b += 2 * C + C + sizeof(R) * nt;    // scr[2], esv, skv
+    b += 7 * C + 7 * D2;                // kf (RF), ka (FP64)
+    b += 2 * D2 + D2 + 8 * (size_t)nt;  // scr[2], esv, skv
     b += (size_t)K * (D2 + C);          // checkpoints
     b += 16 * (size_t)stepcap;          // step log
     b += (size_t)segcap * 5 * C;        // recompute segment
@@ -184,27 +184,27 @@ char* carve(char*& p, size_t bytes) {
 
 // Allocate a workspace for B slots; descriptors point into it.  Caller
 // buffers (u0 etc.) are per-slot arrays inside the workspace.
-template <typename R>
 int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
+    const size_t rf = pr->precision == FL_PRECISION_FP64 ? 8 : 4;
     fl_ctx* ctx = pr->ctx;
     auto w = std::make_unique<Work>();
     w->ctx = ctx;
     w->B = B;
     w->nt = pr->nt;
-    w->rsize = sizeof(R);
+    w->rsize = (int)rf;
     w->K = ctx->opts.checkpoints;
     w->segcap = ctx->opts.segment_steps;
     w->stepcap = ctx->opts.step_log;
     w->nsave = nsave;
     const int nt = pr->nt;
-    const size_t per = slot_bytes<R>(nt, w->K, w->segcap, w->stepcap);
+    const size_t per = slot_bytes(nt, rf, w->K, w->segcap, w->stepcap);
     const size_t io = 16 * (size_t)nt * (2 + nsave + 2) + 8 * (size_t)nt + 256 * 8;
     w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + nt + 4096;
     if (ctx->opts.hbm_budget_bytes && w->pool_bytes > ctx->opts.hbm_budget_bytes)
         return set_err(ctx, FL_OOM_ADMISSION, "workspace of %zu bytes exceeds the HBM budget",
                        w->pool_bytes);
     CU(cudaMalloc(&w->pool, w->pool_bytes));
-    CU(cudaMalloc(&w->d_desc, sizeof(SlotDesc<R>) * B));
+    CU(cudaMalloc(&w->d_desc, sizeof(SlotDesc) * B));
     CU(cudaMalloc(&w->d_state, sizeof(SlotState) * B));
     CU(cudaMalloc(&w->d_active, sizeof(int) * B));
     char* p = w->pool;
@@ -216,16 +216,18 @@ int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
     w->d_uL = (double*)carve(p, 16 * (size_t)nt * B);
     w->d_grad = (double*)carve(p, 8 * (size_t)nt * B);
     w->d_save = nsave ? (double*)carve(p, 16 * (size_t)nt * nsave * B) : nullptr;
-    w->h_desc.resize(sizeof(SlotDesc<R>) * B);
-    SlotDesc<R>* hd = reinterpret_cast<SlotDesc<R>*>(w->h_desc.data());
-    const size_t C = 2 * sizeof(R) * nt, D2 = 16 * (size_t)nt;
+    w->h_desc.resize(sizeof(SlotDesc) * B);
+    SlotDesc* hd = reinterpret_cast<SlotDesc*>(w->h_desc.data());
+    const size_t C = 2 * rf * nt, D2 = 16 * (size_t)nt;
     for (int b = 0; b < B; b++) {
-        SlotDesc<R>& d = hd[b];
+        SlotDesc& d = hd[b];
         memset(&d, 0, sizeof d);
         d.Dturns = pr->d_Dturns;
-        d.Heff = pr->d_Heff;
-        d.ss = pr->d_ss;
-        d.tw = pr->d_tw;
+        for (int q = 0; q < 2; q++) {
+            d.Heff[q] = pr->d_Heff[q];
+            d.ss[q] = pr->d_ss[q];
+            d.tw[q] = pr->d_tw[q];
+        }
         d.gamma = pr->gamma0;
         d.one_m_fR = pr->one_m_fR;
         d.L = pr->L;
@@ -250,11 +252,11 @@ int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
         d.lam[0] = (double*)carve(p, D2);
         d.lam[1] = (double*)carve(p, D2);
         for (int i = 0; i < 7; i++) d.kf[i] = carve(p, C);
-        for (int i = 0; i < 7; i++) d.ka[i] = carve(p, C);
-        d.scr[0] = carve(p, C);
-        d.scr[1] = carve(p, C);
-        d.esv = carve(p, C);
-        d.skv = carve(p, sizeof(R) * nt);
+        for (int i = 0; i < 7; i++) d.ka[i] = carve(p, D2);
+        d.scr[0] = carve(p, D2);
+        d.scr[1] = carve(p, D2);
+        d.esv = (double*)carve(p, D2);
+        d.skv = (double*)carve(p, 8 * (size_t)nt);
         d.ck_u = (double*)carve(p, D2 * w->K);
         d.ck_k1 = carve(p, C * w->K);
         d.steplog = (double*)carve(p, 16 * (size_t)w->stepcap);
@@ -331,11 +333,9 @@ int check_problem(fl_problem* pr) {
 }
 
 template <typename R>
-int upload_tables(fl_problem* pr, const double* D, const double* hR, const double* ss) {
+int upload_table_set(fl_problem* pr, const double* hR, const double* ss, int q) {
     fl_ctx* ctx = pr->ctx;
-    const int nt = pr->nt, m = pr->m;
-    std::vector<double> dturn((size_t)nt * m);
-    for (size_t i = 0; i < dturn.size(); i++) dturn[i] = D[i] / (2.0 * M_PI);
+    const int nt = pr->nt;
     std::vector<R> heff(2 * (size_t)nt), ssv(nt), tw(2 * (size_t)nt);
     for (int k = 0; k < nt; k++) {
         const double sg = (k & 1) ? -1.0 : 1.0;  // fftshift folded into the response
@@ -346,16 +346,27 @@ int upload_tables(fl_problem* pr, const double* D, const double* hR, const doubl
         tw[2 * k] = (R)std::cos(a);
         tw[2 * k + 1] = (R)std::sin(a);
     }
+    CU(cudaMalloc(&pr->d_Heff[q], sizeof(R) * heff.size()));
+    CU(cudaMalloc(&pr->d_ss[q], sizeof(R) * ssv.size()));
+    CU(cudaMalloc(&pr->d_tw[q], sizeof(R) * tw.size()));
+    CU(cudaMemcpy(pr->d_Heff[q], heff.data(), sizeof(R) * heff.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_ss[q], ssv.data(), sizeof(R) * ssv.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_tw[q], tw.data(), sizeof(R) * tw.size(), cudaMemcpyHostToDevice));
+    return FL_OK;
+}
+
+// both precisions of the spectral tables (the adjoint is FP64 in every mode)
+int upload_tables(fl_problem* pr, const double* D, const double* hR, const double* ss) {
+    fl_ctx* ctx = pr->ctx;
+    const int nt = pr->nt, m = pr->m;
+    std::vector<double> dturn((size_t)nt * m);
+    for (size_t i = 0; i < dturn.size(); i++) dturn[i] = D[i] / (2.0 * M_PI);
     CU(cudaMalloc(&pr->d_Dturns, sizeof(double) * dturn.size()));
-    CU(cudaMalloc(&pr->d_Heff, sizeof(R) * heff.size()));
-    CU(cudaMalloc(&pr->d_ss, sizeof(R) * ssv.size()));
-    CU(cudaMalloc(&pr->d_tw, sizeof(R) * tw.size()));
     CU(cudaMemcpy(pr->d_Dturns, dturn.data(), sizeof(double) * dturn.size(),
                   cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(pr->d_Heff, heff.data(), sizeof(R) * heff.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(pr->d_ss, ssv.data(), sizeof(R) * ssv.size(), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(pr->d_tw, tw.data(), sizeof(R) * tw.size(), cudaMemcpyHostToDevice));
-    return FL_OK;
+    int rc = upload_table_set<float>(pr, hR, ss, 0);
+    if (rc) return rc;
+    return upload_table_set<double>(pr, hR, ss, 1);
 }
 
 int status_of_slots(fl_ctx* ctx, const std::vector<SlotState>& st) {
@@ -366,22 +377,15 @@ int status_of_slots(fl_ctx* ctx, const std::vector<SlotState>& st) {
 }
 
 int new_work(fl_problem* pr, int B, int nsave, int mode, Work** w) {
-    return pr->precision == FL_PRECISION_FP64 ? work_create<double>(pr, B, nsave, mode, w)
-                                              : work_create<float>(pr, B, nsave, mode, w);
+    return work_create(pr, B, nsave, mode, w);
 }
 
 // rewrite the mode of every descriptor (host image + device copy)
 int set_mode(fl_ctx* ctx, Work* w, int mode, int log_cost) {
-    const size_t dsz = w->rsize == 8 ? sizeof(SlotDesc<double>) : sizeof(SlotDesc<float>);
     for (int b = 0; b < w->B; b++) {
-        unsigned char* base = w->h_desc.data() + (size_t)b * dsz;
-        if (w->rsize == 8) {
-            reinterpret_cast<SlotDesc<double>*>(base)->mode = mode;
-            reinterpret_cast<SlotDesc<double>*>(base)->log_cost = log_cost;
-        } else {
-            reinterpret_cast<SlotDesc<float>*>(base)->mode = mode;
-            reinterpret_cast<SlotDesc<float>*>(base)->log_cost = log_cost;
-        }
+        SlotDesc* d = reinterpret_cast<SlotDesc*>(w->h_desc.data()) + b;
+        d->mode = mode;
+        d->log_cost = log_cost;
     }
     CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), w->h_desc.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -527,8 +531,7 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
     pr->gamma0 = gamma[0];
     pr->gamma_sym = gamma_symmetric(gamma, m);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
-    int rc = precision == FL_PRECISION_FP64 ? upload_tables<double>(pr.get(), D, hR, selfsteep)
-                                            : upload_tables<float>(pr.get(), D, hR, selfsteep);
+    int rc = upload_tables(pr.get(), D, hR, selfsteep);
     if (rc) {
         fl_problem_destroy(pr.release());
         return rc;
@@ -541,9 +544,11 @@ int fl_problem_destroy(fl_problem* pr) {
     if (!pr) return FL_EINVAL;
     delete pr->last;
     cudaFree(pr->d_Dturns);
-    cudaFree(pr->d_Heff);
-    cudaFree(pr->d_ss);
-    cudaFree(pr->d_tw);
+    for (int q = 0; q < 2; q++) {
+        cudaFree(pr->d_Heff[q]);
+        cudaFree(pr->d_ss[q]);
+        cudaFree(pr->d_tw[q]);
+    }
     delete pr;
     return FL_OK;
 }

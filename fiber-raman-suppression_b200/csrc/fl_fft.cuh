@@ -142,64 +142,151 @@ struct FftShape {
     static constexpr int NPASS = NFULL + (REM > 0 ? 1 : 0);
 };
 
-// One Stockham pass of radix RP with stride ns (the product of the previous
-// radices).  FIRST: inputs come from registers; LAST: outputs stay in
-// registers.  Between passes the data goes through the padded smem buffer.
-template <typename R, int LOGN, int LOGE, int RP, bool FIRST, bool LAST, bool INV>
-__device__ __forceinline__ void stockham_pass(cx<R> (&v)[1 << LOGE], cx<R>* __restrict__ sm,
-                                              const cx<R>* __restrict__ tw, const int ns) {
+// The smem exchange moves whole complex values through one padded buffer,
+// or -- when that buffer would not fit in shared memory (FP64 at 2^14
+// points) -- the real and the imaginary parts in two rounds through a buffer
+// of half the size.
+template <typename R, int LOGN>
+struct SmemPlan {
+    static constexpr bool SPLIT = sizeof(R) * 2 * (size_t)padded_len(1 << LOGN) > 200 * 1024;
+    static constexpr size_t BYTES =
+        (SPLIT ? sizeof(R) : 2 * sizeof(R)) * (size_t)padded_len(1 << LOGN);
+};
+
+// Twiddles and radix-RP DFTs of one Stockham pass with stride ns (the product
+// of the previous radices) on the E values of this thread.  The first pass
+// (ns = 1) has no twiddles.
+template <typename R, int LOGN, int LOGE, int RP, bool FIRST>
+__device__ __forceinline__ void pass_compute(cx<R> (&v)[1 << LOGE], const cx<R>* __restrict__ tw,
+                                             const int ns) {
     using S = FftShape<LOGN, LOGE>;
     constexpr int E = S::E, T = S::T, N = S::N;
     constexpr int BPT = E / RP;  // butterflies per thread
     const int t = threadIdx.x;
-    if constexpr (!FIRST) {
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = sm[pad(t + T * s)];
-        __syncthreads();
-    }
     const int tws = N / (ns * RP);
 #pragma unroll
     for (int q = 0; q < BPT; q++) {
-        const int j = t + T * q;
-        const int m = j & (ns - 1);
         if constexpr (!FIRST) {
+            const int m = (t + T * q) & (ns - 1);
+            if constexpr (sizeof(R) == 8) {
+                // FP64: powers of one table twiddle (rounding stays ~1e-15)
+                const cx<R> w1 = tw[m * tws];
+                cx<R> w = w1;
 #pragma unroll
-            for (int r = 1; r < RP; r++) {
-                cx<R> w = tw[m * r * tws];
-                if (INV) w.im = -w.im;
-                v[q + BPT * r] = cmul(v[q + BPT * r], w);
+                for (int r = 1; r < RP; r++) {
+                    v[q + BPT * r] = cmul(v[q + BPT * r], w);
+                    if (r + 1 < RP) w = cmul(w, w1);
+                }
+            } else {
+                // FP32: every twiddle from the correctly rounded table
+#pragma unroll
+                for (int r = 1; r < RP; r++) v[q + BPT * r] = cmul(v[q + BPT * r], tw[m * r * tws]);
             }
         }
-        dft_inreg<RP, INV, BPT>(v, q);
-        if constexpr (!LAST) {
-            const int base = (j - m) * RP + m;
+        dft_inreg<RP, false, BPT>(v, q);
+    }
+}
+
+// Stockham reordering between passes: the outputs of a radix-RP pass with
+// stride ns go to positions (j - m) RP + m + r ns; the next pass reads
+// positions t + T s.  All threads of the block call it.
+template <typename R, int LOGN, int LOGE, int RP>
+__device__ __forceinline__ void pass_exchange(cx<R> (&v)[1 << LOGE], void* __restrict__ smv,
+                                              const int ns) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int E = S::E, T = S::T;
+    constexpr int BPT = E / RP;
+    const int t = threadIdx.x;
+    if constexpr (!SmemPlan<R, LOGN>::SPLIT) {
+        cx<R>* sm = (cx<R>*)smv;
+#pragma unroll
+        for (int q = 0; q < BPT; q++) {
+            const int j = t + T * q, m = j & (ns - 1), base = (j - m) * RP + m;
 #pragma unroll
             for (int r = 0; r < RP; r++) sm[pad(base + r * ns)] = v[q + BPT * r];
         }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = sm[pad(t + T * s)];
+        __syncthreads();
+    } else {
+        R* sm = (R*)smv;
+#pragma unroll
+        for (int part = 0; part < 2; part++) {
+#pragma unroll
+            for (int q = 0; q < BPT; q++) {
+                const int j = t + T * q, m = j & (ns - 1), base = (j - m) * RP + m;
+#pragma unroll
+                for (int r = 0; r < RP; r++)
+                    sm[pad(base + r * ns)] = part ? v[q + BPT * r].im : v[q + BPT * r].re;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                if (part) v[s].im = sm[pad(t + T * s)];
+                else v[s].re = sm[pad(t + T * s)];
+            }
+            __syncthreads();
+        }
     }
-    if constexpr (!LAST) __syncthreads();
 }
 
-// Block-wide unnormalised transform of the N values held in v (all threads
-// of the block must call it).  The passes between the first and the last
-// run as a runtime loop over one code body, so the whole kernel carries one
-// copy of each pass type.  The smem buffer must hold padded_len(N) elements.
-template <typename R, int LOGN, int LOGE, bool INV = false>
-__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], cx<R>* sm, const cx<R>* tw) {
+// out[s] = value at position (N - (t + T s)) mod N of the field held in v
+// (the k <-> -k pairing of two packed real spectra)
+template <typename R, int LOGN, int LOGE>
+__device__ __forceinline__ void gather_negated(const cx<R> (&v)[1 << LOGE], cx<R> (&out)[1 << LOGE],
+                                               void* __restrict__ smv) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int E = S::E, T = S::T, N = S::N;
+    const int t = threadIdx.x;
+    if constexpr (!SmemPlan<R, LOGN>::SPLIT) {
+        cx<R>* sm = (cx<R>*)smv;
+#pragma unroll
+        for (int s = 0; s < E; s++) sm[pad(t + T * s)] = v[s];
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) out[s] = sm[pad((N - (t + T * s)) & (N - 1))];
+        __syncthreads();
+    } else {
+        R* sm = (R*)smv;
+#pragma unroll
+        for (int part = 0; part < 2; part++) {
+#pragma unroll
+            for (int s = 0; s < E; s++) sm[pad(t + T * s)] = part ? v[s].im : v[s].re;
+            __syncthreads();
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const R x = sm[pad((N - (t + T * s)) & (N - 1))];
+                if (part) out[s].im = x;
+                else out[s].re = x;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Block-wide unnormalised forward transform (exponent sign -1) of the N
+// values held in v; all threads of the block call it.  The passes between
+// the first and the last run as a runtime loop over one code body, so a
+// kernel carries one copy of each pass type.
+template <typename R, int LOGN, int LOGE>
+__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], void* sm, const cx<R>* tw) {
     using S = FftShape<LOGN, LOGE>;
     constexpr int E = S::E;
     constexpr int RL = S::REM ? (1 << S::REM) : E;  // radix of the last pass
     if constexpr (S::NPASS == 1) {
-        dft_inreg<E, INV, 1>(v, 0);
+        dft_inreg<E, false, 1>(v, 0);
     } else {
-        stockham_pass<R, LOGN, LOGE, E, true, false, INV>(v, sm, tw, 1);
+        pass_compute<R, LOGN, LOGE, E, true>(v, tw, 1);
+        pass_exchange<R, LOGN, LOGE, E>(v, sm, 1);
         int ns = E;
 #pragma unroll 1
         for (int p = 1; p < S::NPASS - 1; p++) {
-            stockham_pass<R, LOGN, LOGE, E, false, false, INV>(v, sm, tw, ns);
+            pass_compute<R, LOGN, LOGE, E, false>(v, tw, ns);
+            pass_exchange<R, LOGN, LOGE, E>(v, sm, ns);
             ns *= E;
         }
-        stockham_pass<R, LOGN, LOGE, RL, false, true, INV>(v, sm, tw, ns);
+        pass_compute<R, LOGN, LOGE, RL, false>(v, tw, ns);
     }
 }
 

@@ -21,6 +21,14 @@
 // (conj(Heff)).  The two Raman terms of the reference adjoint (:93-132) are
 // complex conjugates of each other and combine into the single real
 // correlation of Y; h∗I and h̃⋆Y share one complex transform pair.
+//
+// Precision: the forward solve and its recompute run in RF (FP32 in the
+// default mode) with FP64 phase arguments, FP64 state accumulation and an FP64
+// error norm; the dense interpolant is stored in RF.  The adjoint integration
+// (the gradient accumulation along z) runs in RA = FP64: an FP32 adjoint
+// amplifies its round-off through the modulation-instability gain of the
+// anomalous-dispersion fiber and misses 1e-3 gradient accuracy (measured
+// 2e-3..7e-3 on the Nt = 2^13 band-objective problem; 4e-6 in FP64).
 #pragma once
 #include "fl_fft.cuh"
 #include "fl_types.h"
@@ -123,14 +131,16 @@ __device__ __forceinline__ double block_max(double v, double* red) {
     return s;
 }
 
+// Block-level pieces of one problem's solve in RHS precision R.
 template <typename R, int LOGN, int LOGE>
 struct SmSolver {
     using S = FftShape<LOGN, LOGE>;
     static constexpr int N = S::N, E = S::E, T = S::T;
+    static constexpr int P = sizeof(R) == 8 ? 1 : 0;  // table precision index
     using C = cx<R>;
 
-    const SlotDesc<R>& d;
-    C* sm;          // padded transform buffer
+    const SlotDesc& d;
+    void* sm;       // padded transform buffer
     double* red;    // 32 doubles
     const C* tw;
     const C* Heff;
@@ -138,9 +148,9 @@ struct SmSolver {
     C* scr0;
     C* scr1;
 
-    __device__ SmSolver(const SlotDesc<R>& dd, C* smem, double* r)
-        : d(dd), sm(smem), red(r), tw((const C*)dd.tw), Heff((const C*)dd.Heff),
-          ss((const R*)dd.ss), scr0((C*)dd.scr[0]), scr1((C*)dd.scr[1]) {}
+    __device__ SmSolver(const SlotDesc& dd, void* smem, double* r)
+        : d(dd), sm(smem), red(r), tw((const C*)dd.tw[P]), Heff((const C*)dd.Heff[P]),
+          ss((const R*)dd.ss[P]), scr0((C*)dd.scr[0]), scr1((C*)dd.scr[1]) {}
 
     __device__ __forceinline__ static int bin(int s) { return threadIdx.x + T * s; }
 
@@ -208,19 +218,16 @@ struct SmSolver {
                 }
             } else if (op == 11) {
                 // split the two real spectra with X[k] and conj(X[-k])
-#pragma unroll
-                for (int s = 0; s < E; s++) sm[pad(bin(s))] = v[s];
-                __syncthreads();
+                C xm[E];
+                gather_negated<R, LOGN, LOGE>(v, xm, sm);
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = bin(s);
-                    const C zm = conjc(sm[pad((N - b) & (N - 1))]);
-                    const C H = Heff[b];
+                    const C zm = conjc(xm[s]);
+                    const C H = Heff[bin(s)];
                     const C a = scale(v[s] + zm, R(0.5));   // spectrum of I
                     const C c = scale(v[s] - zm, R(0.5));   // i * spectrum of Y
                     v[s] = cmul(a, H) + cmulc(c, H);
                 }
-                __syncthreads();
                 inv = true;
             } else {  // op == 12
 #pragma unroll
@@ -230,7 +237,7 @@ struct SmSolver {
                     const R I = g * abs2(ut);
                     const R Rr = v[s].re * invn, Ri = v[s].im * invn;
                     const C t1 = scale(lt, R(2) * ofr * I + Rr);
-                    const C t2 = scale(cmulc(cmul(ut, ut), lt), ofr * g);  // (1-fR)γ λ* u²
+                    const C t2 = scale(cmulc(cmul(ut, ut), lt), ofr * g);    // (1-fR)γ λ* u²
                     const C t3 = mk(-R(2) * Ri * ut.im, R(2) * Ri * ut.re);  // 2i Ri u
                     v[s] = t1 - t2 + t3;
                 }
@@ -250,8 +257,8 @@ struct SmSolver {
     }
 
     // ---- stage helpers ---------------------------------------------------
+    // logical stage i -> physical buffer; perm swaps stages 0 and 6 (FSAL)
     __device__ __forceinline__ static C* kp(void* const (&k)[7], int perm, int i) {
-        // logical stage i -> physical buffer; perm swaps stages 0 and 6 (FSAL)
         int p = (perm && (i == 0 || i == 6)) ? 6 - i : i;
         return (C*)k[p];
     }
@@ -280,8 +287,6 @@ struct SmSolver {
                                                  void* const (&k)[7], int perm, double dt,
                                                  double abstol, double reltol, C (&v)[E],
                                                  bool want_err) {
-        C* esv = (C*)d.esv;
-        R* skv = (R*)d.skv;
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int b = bin(s);
@@ -298,10 +303,10 @@ struct SmSolver {
             const cx<double> u1 = mk(un.re + dt * ar, un.im + dt * ai);
             st2(unew, b, u1);
             if (want_err) {
-                esv[b] = mk((R)(dt * er), (R)(dt * ei));
+                st2(d.esv, b, mk(dt * er, dt * ei));
                 const double m0 = sqrt(un.re * un.re + un.im * un.im);
                 const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
-                skv[b] = (R)(abstol + fmax(m0, m1) * reltol);
+                d.skv[b] = abstol + fmax(m0, m1) * reltol;
             }
             v[s] = down<R>(u1);
         }
@@ -309,40 +314,43 @@ struct SmSolver {
 
     // finish the error estimate with k7 (in v) -> EEst (block-uniform)
     __device__ __forceinline__ double error_norm(const C (&k7)[E], double dt) {
-        const C* esv = (const C*)d.esv;
-        const R* skv = (const R*)d.skv;
         const double bt7 = kT5bt[6];
         double acc = 0.0;
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int b = bin(s);
-            const C e6 = esv[b];
-            const double er = (double)e6.re + dt * bt7 * (double)k7[s].re;
-            const double ei = (double)e6.im + dt * bt7 * (double)k7[s].im;
-            const double w = 1.0 / (double)skv[b];
-            acc += (er * er + ei * ei) * (w * w);
+            const cx<double> e6 = ld2(d.esv, b);
+            const double er = e6.re + dt * bt7 * (double)k7[s].re;
+            const double ei = e6.im + dt * bt7 * (double)k7[s].im;
+            const double w = d.skv[b];
+            acc += (er * er + ei * ei) / (w * w);
         }
         const double tot = block_sum<T>(acc, red);
         return sqrt(tot / (double)N);
     }
-
-    // dense interpolant of a stored forward step at θ, into w
-    __device__ __forceinline__ void interp(int slot, double dtn, double th, C (&w)[E]) {
-        const C* sg = (const C*)d.seg + (size_t)slot * 5 * N;
-        const double t2 = th * th, t3 = t2 * th, t4 = t3 * th;
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            const C c0 = sg[b], c1 = sg[N + b], c2 = sg[2 * N + b], c3 = sg[3 * N + b],
-                    c4 = sg[4 * N + b];
-            const double xr = (double)c0.re + dtn * (th * (double)c1.re + t2 * (double)c2.re +
-                                                     t3 * (double)c3.re + t4 * (double)c4.re);
-            const double xi = (double)c0.im + dtn * (th * (double)c1.im + t2 * (double)c2.im +
-                                                     t3 * (double)c3.im + t4 * (double)c4.im);
-            w[s] = mk((R)xr, (R)xi);
-        }
-    }
 };
+
+// dense interpolant of a stored forward step (precision RF) at θ, into a
+// field of precision R
+template <typename RF, typename R, int LOGN, int LOGE>
+__device__ __forceinline__ void interp_step(const SlotDesc& d, int slot, double dtn, double th,
+                                            cx<R> (&w)[FftShape<LOGN, LOGE>::E]) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int N = S::N, E = S::E, T = S::T;
+    const cx<RF>* sg = (const cx<RF>*)d.seg + (size_t)slot * 5 * N;
+    const double t2 = th * th, t3 = t2 * th, t4 = t3 * th;
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int b = threadIdx.x + T * s;
+        const cx<RF> c0 = sg[b], c1 = sg[N + b], c2 = sg[2 * N + b], c3 = sg[3 * N + b],
+                     c4 = sg[4 * N + b];
+        const double xr = (double)c0.re + dtn * (th * (double)c1.re + t2 * (double)c2.re +
+                                                 t3 * (double)c3.re + t4 * (double)c4.re);
+        const double xi = (double)c0.im + dtn * (th * (double)c1.im + t2 * (double)c2.im +
+                                                 t3 * (double)c3.im + t4 * (double)c4.im);
+        w[s] = mk((R)xr, (R)xi);
+    }
+}
 
 // PI controller: returns q and q11 (OrdinaryDiffEqCore stepsize_controller!)
 __device__ __forceinline__ double pi_q(double EEst, double qold, double& q11) {
@@ -370,24 +378,27 @@ __device__ __forceinline__ double initdt_final(double dt0, double d1, double d2,
     return fmax(dtmin, fmin(fmin(100 * dt0, dt1), span));
 }
 
-template <typename R, int LOGN, int LOGE>
+// Forward field for the adjoint RHS: the dense interpolant of the stored step
+// of the current segment that holds zz, or an FP64 field given directly.
+template <typename RF, typename R, int LOGN, int LOGE>
 struct SegLoader {
-    using Sol = SmSolver<R, LOGN, LOGE>;
-    Sol& S;
+    static constexpr int E = FftShape<LOGN, LOGE>::E;
+    const SlotDesc& d;
     int seg_lo, seg_hi;
     double zz;
-    const double* direct;  // FP64 field given directly (single RHS evaluations)
-    __device__ void operator()(cx<R> (&w)[Sol::E]) const {
+    const double* direct;
+    __device__ void operator()(cx<R> (&w)[E]) const {
         if (direct) {
 #pragma unroll
-            for (int s = 0; s < Sol::E; s++) w[s] = down<R>(ld2(direct, Sol::bin(s)));
+            for (int s = 0; s < E; s++)
+                w[s] = down<R>(ld2(direct, threadIdx.x + FftShape<LOGN, LOGE>::T * s));
             return;
         }
-        const double* lg = S.d.steplog;
+        const double* lg = d.steplog;
         int n = seg_lo;
         while (n + 1 < seg_hi && lg[2 * (n + 1)] <= zz) n++;
         const double zn = lg[2 * n], dtn = lg[2 * n + 1];
-        S.interp(n - seg_lo, dtn, (zz - zn) / dtn, w);
+        interp_step<RF, R, LOGN, LOGE>(d, n - seg_lo, dtn, (zz - zn) / dtn, w);
     }
 };
 
@@ -395,7 +406,7 @@ struct SegLoader {
 // budget of the CTA instead of sharing it with the state machine's live
 // values; the 2E-register field crosses the call through local memory.
 template <typename R, int LOGN, int LOGE>
-__device__ __noinline__ void rhs_fwd_call(const SlotDesc<R>* d, cx<R>* sm, double* red, double z,
+__device__ __noinline__ void rhs_fwd_call(const SlotDesc* d, void* sm, double* red, double z,
                                           cx<R>* vio) {
     using Sol = SmSolver<R, LOGN, LOGE>;
     Sol S(*d, sm, red);
@@ -407,10 +418,8 @@ __device__ __noinline__ void rhs_fwd_call(const SlotDesc<R>* d, cx<R>* sm, doubl
     for (int s = 0; s < Sol::E; s++) vio[s] = v[s];
 }
 
-// ufwd != nullptr: the forward field is read from that FP64 buffer (single
-// RHS evaluations); otherwise from the dense interpolant of the segment
-template <typename R, int LOGN, int LOGE>
-__device__ __noinline__ void rhs_adj_call(const SlotDesc<R>* d, cx<R>* sm, double* red, double z,
+template <typename RF, typename R, int LOGN, int LOGE>
+__device__ __noinline__ void rhs_adj_call(const SlotDesc* d, void* sm, double* red, double z,
                                           cx<R>* vio, int seg_lo, int seg_hi, double zload,
                                           const double* ufwd) {
     using Sol = SmSolver<R, LOGN, LOGE>;
@@ -418,46 +427,55 @@ __device__ __noinline__ void rhs_adj_call(const SlotDesc<R>* d, cx<R>* sm, doubl
     cx<R> v[Sol::E];
 #pragma unroll
     for (int s = 0; s < Sol::E; s++) v[s] = vio[s];
-    SegLoader<R, LOGN, LOGE> ld{S, seg_lo, seg_hi, zload, ufwd};
+    SegLoader<RF, R, LOGN, LOGE> ld{*d, seg_lo, seg_hi, zload, ufwd};
     S.rhs(true, z, v, ld);
 #pragma unroll
     for (int s = 0; s < Sol::E; s++) vio[s] = v[s];
 }
 
-// One RHS evaluation on one CTA (unit parity of the right-hand sides):
-// in/ufwd/out are N complex doubles.
-template <typename R, int LOGN, int LOGE>
-__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
-    sm_rhs_kernel(const SlotDesc<R>* __restrict__ d, int adjoint, double z,
-                  const double* __restrict__ in, const double* __restrict__ ufwd,
-                  double* __restrict__ out) {
-    using Sol = SmSolver<R, LOGN, LOGE>;
-    using C = cx<R>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
-    double* red = reinterpret_cast<double*>(smraw + sizeof(C) * padded_len(Sol::N));
-    C v[Sol::E];
-#pragma unroll
-    for (int s = 0; s < Sol::E; s++) v[s] = down<R>(ld2(in, Sol::bin(s)));
-    if (adjoint)
-        rhs_adj_call<R, LOGN, LOGE>(d, sm, red, z, v, 0, 0, 0.0, ufwd);
-    else
-        rhs_fwd_call<R, LOGN, LOGE>(d, sm, red, z, v);
-#pragma unroll
-    for (int s = 0; s < Sol::E; s++) st2(out, Sol::bin(s), up(v[s]));
+// transform buffer (sized for the adjoint precision) + 32 reduction doubles
+template <typename RA, int LOGN>
+constexpr size_t smem_bytes() {
+    return SmemPlan<RA, LOGN>::BYTES + 32 * sizeof(double);
 }
 
-template <typename R, int LOGN, int LOGE>
-__device__ __forceinline__ void restore_checkpoint(const SlotDesc<R>& d, int seg, SlotState& st) {
-    using Sol = SmSolver<R, LOGN, LOGE>;
-    using C = cx<R>;
-    constexpr int N = Sol::N, E = Sol::E;
+// One RHS evaluation on one CTA (unit parity of the right-hand sides):
+// in/ufwd/out are N complex doubles; forward in RF, adjoint in RA.
+template <typename RF, typename RA, int LOGN, int LOGE>
+__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+    sm_rhs_kernel(const SlotDesc* __restrict__ d, int adjoint, double z,
+                  const double* __restrict__ in, const double* __restrict__ ufwd,
+                  double* __restrict__ out) {
+    using S = FftShape<LOGN, LOGE>;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    double* red = reinterpret_cast<double*>(smraw + SmemPlan<RA, LOGN>::BYTES);
+    if (adjoint) {
+        cx<RA> v[S::E];
+#pragma unroll
+        for (int s = 0; s < S::E; s++) v[s] = down<RA>(ld2(in, threadIdx.x + S::T * s));
+        rhs_adj_call<RF, RA, LOGN, LOGE>(d, smraw, red, z, v, 0, 0, 0.0, ufwd);
+#pragma unroll
+        for (int s = 0; s < S::E; s++) st2(out, threadIdx.x + S::T * s, up(v[s]));
+    } else {
+        cx<RF> v[S::E];
+#pragma unroll
+        for (int s = 0; s < S::E; s++) v[s] = down<RF>(ld2(in, threadIdx.x + S::T * s));
+        rhs_fwd_call<RF, LOGN, LOGE>(d, smraw, red, z, v);
+#pragma unroll
+        for (int s = 0; s < S::E; s++) st2(out, threadIdx.x + S::T * s, up(v[s]));
+    }
+}
+
+template <typename RF, int LOGN, int LOGE>
+__device__ __forceinline__ void restore_checkpoint(const SlotDesc& d, int seg, SlotState& st) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int N = S::N, E = S::E, T = S::T;
 #pragma unroll
     for (int s = 0; s < E; s++) {
-        const int b = Sol::bin(s);
+        const int b = threadIdx.x + T * s;
         reinterpret_cast<double2*>(d.u[0])[b] =
             reinterpret_cast<const double2*>(d.ck_u)[(size_t)seg * N + b];
-        ((C*)d.kf[0])[b] = ((const C*)d.ck_k1)[(size_t)seg * N + b];
+        ((cx<RF>*)d.kf[0])[b] = ((const cx<RF>*)d.ck_k1)[(size_t)seg * N + b];
     }
     st.cur = 0;
     st.kperm = 0;
@@ -465,24 +483,83 @@ __device__ __forceinline__ void restore_checkpoint(const SlotDesc<R>& d, int seg
     st.stage = 0;
 }
 
-template <typename R, int LOGN, int LOGE>
+// Hairer initial step, part 1 (after f0): stores f0 as the FSAL derivative,
+// returns the probe step dt0 (> 0) or, when no probe is needed, -dtinit.
+template <typename K, int LOGN, int LOGE>
+__device__ __forceinline__ double init_after_f0(const double* x0, cx<K>* k1, const cx<K>* v,
+                                                double at, double rt, double L, double dtmin,
+                                                double* red, double& d1_out) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int N = S::N, E = S::E, T = S::T;
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int b = threadIdx.x + T * s;
+        k1[b] = v[s];
+        const cx<double> x = ld2(x0, b);
+        const double ax = sqrt(x.re * x.re + x.im * x.im);
+        const double sk = at + ax * rt;
+        s0 += (ax / sk) * (ax / sk);
+        const double af = sqrt(abs2(up(v[s])));
+        s1 += (af / sk) * (af / sk);
+    }
+    const double d0 = sqrt(block_sum<T>(s0, red) / N);
+    const double d1 = sqrt(block_sum<T>(s1, red) / N);
+    d1_out = d1;
+    const double dt0 = initdt_first(d0, d1, L);
+    if (!isfinite(d1)) return -dtmin;
+    if (dt0 < 10 * kEps) return -fmax(1e-6, dtmin);
+    return dt0;
+}
+
+// Hairer initial step, part 2 (after the probe f1 at x0 ± dt0 f0)
+template <typename K, int LOGN, int LOGE>
+__device__ __forceinline__ double init_after_f1(const double* x0, const cx<K>* k1, const cx<K>* v,
+                                                double at, double rt, double dt0, double d1,
+                                                double L, double dtmin, double* red) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int N = S::N, E = S::E, T = S::T;
+    double s2 = 0.0, ndiff = 0.0;
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int b = threadIdx.x + T * s;
+        const cx<double> x = ld2(x0, b);
+        const double sk = at + sqrt(x.re * x.re + x.im * x.im) * rt;
+        const cx<K> f0 = k1[b];
+        const double dr = (double)v[s].re - (double)f0.re;
+        const double di = (double)v[s].im - (double)f0.im;
+        s2 += (dr * dr + di * di) / (sk * sk);
+        ndiff += (dr != 0.0 || di != 0.0) ? 1.0 : 0.0;
+    }
+    const double d2 = sqrt(block_sum<T>(s2, red) / N) / dt0;
+    const double nd = block_sum<T>(ndiff, red);
+    return initdt_final(dt0, d1, d2, nd, dtmin, L);
+}
+
+// The state machine.  Each loop iteration performs at most one RHS
+// evaluation (forward in RF, adjoint in RA) plus the bookkeeping around it,
+// so the FFT code exists once per precision in the kernel.
+template <typename RF, typename RA, int LOGN, int LOGE>
 __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
-    sm_advance_kernel(const SlotDesc<R>* __restrict__ descs, SlotState* __restrict__ states,
+    sm_advance_kernel(const SlotDesc* __restrict__ descs, SlotState* __restrict__ states,
                       const int* __restrict__ active, int max_evals) {
-    using Sol = SmSolver<R, LOGN, LOGE>;
-    using C = cx<R>;
-    constexpr int N = Sol::N, E = Sol::E, T = Sol::T;
+    using SolF = SmSolver<RF, LOGN, LOGE>;
+    using SolA = SmSolver<RA, LOGN, LOGE>;
+    using CF = cx<RF>;
+    using CA = cx<RA>;
+    constexpr int N = SolF::N, E = SolF::E, T = SolF::T;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
-    double* red = reinterpret_cast<double*>(smraw + sizeof(C) * padded_len(N));
+    double* red = reinterpret_cast<double*>(smraw + SmemPlan<RA, LOGN>::BYTES);
 
     const int slot = active[blockIdx.x];
-    const SlotDesc<R>& d = descs[slot];
+    const SlotDesc& d = descs[slot];
     SlotState st = states[slot];  // block-uniform copy
-    Sol S(d, sm, red);
+    SolF SF(d, smraw, red);
+    SolA SA(d, smraw, red);
     const int tid = threadIdx.x;
     const double L = d.L, dtmin = kEps * L;
-    C v[E];
+    CF vf[E];
+    CA va[E];
     int evals = 0;
 
     while (st.phase != PH_DONE && evals < max_evals) {
@@ -495,7 +572,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 double et = 0.0, eb = 0.0;
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
+                    const int b = SolF::bin(s);
                     const cx<double> x = ld2(uf, b);
                     const double e = x.re * x.re + x.im * x.im;
                     et += e;
@@ -513,7 +590,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 // e^{-iDL} (u_L (mask - J)/E) = ũ(L) (mask - J)/E
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
+                    const int b = SolF::bin(s);
                     const cx<double> x = ld2(uf, b);
                     const double f = ((d.mask[b] ? 1.0 : 0.0) - cost) * sc;
                     st2(lam, b, mk(x.re * f, x.im * f));
@@ -522,7 +599,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 st.J = 0.0;
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
+                    const int b = SolF::bin(s);
                     const cx<double> x = ld2(d.lamL, b);
                     const cx<double> p = phasor<double>(d.Dturns[b], L);
                     st2(lam, b, mk(x.re * p.re + x.im * p.im, x.im * p.re - x.re * p.im));
@@ -532,7 +609,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             bool finite = true;
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const cx<double> x = ld2(lam, Sol::bin(s));
+                const cx<double> x = ld2(lam, SolF::bin(s));
                 const double a = sqrt(x.re * x.re + x.im * x.im);
                 if (!isfinite(a)) finite = false;
                 mx = fmax(mx, a);
@@ -553,7 +630,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             st.acur = 0;
             st.akperm = 0;
             st.a_naccept = st.a_nreject = st.a_nf = st.a_iters = 0;
-            restore_checkpoint<R, LOGN, LOGE>(d, st.seg, st);
+            restore_checkpoint<RF, LOGN, LOGE>(d, st.seg, st);
             st.phase = PH_REC;
             continue;
         }
@@ -562,7 +639,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double* lam = d.lam[st.acur];
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const int b = Sol::bin(s);
+                const int b = SolF::bin(s);
                 const cx<double> l = ld2(lam, b);
                 if (d.lam0_out) st2(d.lam0_out, b, l);
                 if (d.grad_out) {
@@ -578,17 +655,18 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         const bool adj = st.phase == PH_ADJ_INIT || st.phase == PH_ADJ;
         double ze = 0.0, zload = 0.0;
         if (st.phase == PH_FWD_INIT) {
-            const C* k1 = (const C*)d.kf[0];
+            const CF* k1 = (const CF*)d.kf[0];
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const int b = Sol::bin(s);
+                const int b = SolF::bin(s);
                 const cx<double> x = ld2(d.u0, b);
                 if (st.stage == 0) {
                     st2(d.u[0], b, x);
-                    v[s] = down<R>(x);
+                    vf[s] = down<RF>(x);
                 } else {
-                    const C f0 = k1[b];
-                    v[s] = mk((R)(x.re + st.cdt * (double)f0.re), (R)(x.im + st.cdt * (double)f0.im));
+                    const CF f0 = k1[b];
+                    vf[s] = mk((RF)(x.re + st.cdt * (double)f0.re),
+                               (RF)(x.im + st.cdt * (double)f0.im));
                 }
             }
             ze = st.stage == 0 ? 0.0 : st.cdt;
@@ -620,23 +698,24 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             }
             const double* u = d.u[st.cur];
             if (st.stage < 6)
-                S.stage_input(st.stage, u, d.kf, st.kperm, st.cdt, v);
+                SF.stage_input(st.stage, u, d.kf, st.kperm, st.cdt, vf);
             else
-                S.stage7_input(u, d.u[st.cur ^ 1], d.kf, st.kperm, st.cdt, d.abstol, d.reltol, v,
-                               st.phase == PH_FWD);
+                SF.stage7_input(u, d.u[st.cur ^ 1], d.kf, st.kperm, st.cdt, d.abstol, d.reltol,
+                                vf, st.phase == PH_FWD);
             ze = st.cz + kT5c[st.stage] * st.cdt;
         } else if (st.phase == PH_ADJ_INIT) {
             const double* lam = d.lam[0];
-            const C* k1 = (const C*)d.ka[0];
+            const CA* k1 = (const CA*)d.ka[0];
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const int b = Sol::bin(s);
+                const int b = SolF::bin(s);
                 const cx<double> x = ld2(lam, b);
                 if (st.stage == 0) {
-                    v[s] = down<R>(x);
+                    va[s] = down<RA>(x);
                 } else {
-                    const C f0 = k1[b];
-                    v[s] = mk((R)(x.re - st.cdt * (double)f0.re), (R)(x.im - st.cdt * (double)f0.im));
+                    const CA f0 = k1[b];
+                    va[s] = mk((RA)(x.re - st.cdt * (double)f0.re),
+                               (RA)(x.im - st.cdt * (double)f0.im));
                 }
             }
             ze = st.stage == 0 ? L : L - st.cdt;
@@ -666,10 +745,10 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             }
             const double* lam = d.lam[st.acur];
             if (st.stage < 6)
-                S.stage_input(st.stage, lam, d.ka, st.akperm, st.cdt, v);
+                SA.stage_input(st.stage, lam, d.ka, st.akperm, st.cdt, va);
             else
-                S.stage7_input(lam, d.lam[st.acur ^ 1], d.ka, st.akperm, st.cdt, st.abstol_adj,
-                               d.reltol, v, true);
+                SA.stage7_input(lam, d.lam[st.acur ^ 1], d.ka, st.akperm, st.cdt, st.abstol_adj,
+                                d.reltol, va, true);
             ze = zload = st.cz + kT5c[st.stage] * st.cdt;
         }
 
@@ -677,60 +756,38 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         if (adj) {
             const int seg_lo = st.seg * st.ck_stride;
             const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
-            rhs_adj_call<R, LOGN, LOGE>(&d, sm, red, ze, v, seg_lo, seg_hi, zload, nullptr);
+            rhs_adj_call<RF, RA, LOGN, LOGE>(&d, smraw, red, ze, va, seg_lo, seg_hi, zload,
+                                             nullptr);
         } else {
-            rhs_fwd_call<R, LOGN, LOGE>(&d, sm, red, ze, v);
+            rhs_fwd_call<RF, LOGN, LOGE>(&d, smraw, red, ze, vf);
         }
         evals++;
 
         // ------------------------------------------------ consume the derivative
         if (st.phase == PH_FWD_INIT || st.phase == PH_ADJ_INIT) {
             const bool fw = st.phase == PH_FWD_INIT;
-            const double* x0 = fw ? d.u0 : d.lam[0];
-            const double at = fw ? d.abstol : st.abstol_adj, rt = d.reltol;
-            C* k1 = (C*)(fw ? d.kf[0] : d.ka[0]);
             if (st.stage == 0) {
-                double s0 = 0.0, s1 = 0.0;
-#pragma unroll
-                for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
-                    k1[b] = v[s];
-                    const cx<double> x = ld2(x0, b);
-                    const double ax = sqrt(x.re * x.re + x.im * x.im);
-                    const double sk = at + ax * rt;
-                    s0 += (ax / sk) * (ax / sk);
-                    const double af = sqrt(abs2(up(v[s])));
-                    s1 += (af / sk) * (af / sk);
-                }
-                const double d0 = sqrt(block_sum<T>(s0, red) / N);
-                const double d1 = sqrt(block_sum<T>(s1, red) / N);
-                const double dt0 = initdt_first(d0, d1, L);
-                double dtinit = -1.0;
-                if (!isfinite(d1)) dtinit = dtmin;
-                else if (dt0 < 10 * kEps) dtinit = fmax(1e-6, dtmin);
-                if (dtinit < 0.0) {
-                    st.cdt = dt0;  // probe step
+                double d1;
+                const double r = fw ? init_after_f0<RF, LOGN, LOGE>(d.u0, (CF*)d.kf[0], vf,
+                                                                    d.abstol, d.reltol, L, dtmin,
+                                                                    red, d1)
+                                    : init_after_f0<RA, LOGN, LOGE>(d.lam[0], (CA*)d.ka[0], va,
+                                                                    st.abstol_adj, d.reltol, L,
+                                                                    dtmin, red, d1);
+                if (r > 0.0) {  // probe step
+                    st.cdt = r;
                     st.cz = d1;
                     st.stage = 1;
                     continue;
                 }
-                st.cdt = dtinit;
+                st.cdt = -r;
             } else {
-                double s2 = 0.0, ndiff = 0.0;
-#pragma unroll
-                for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
-                    const cx<double> x = ld2(x0, b);
-                    const double sk = at + sqrt(x.re * x.re + x.im * x.im) * rt;
-                    const C f0 = k1[b];
-                    const double dr = (double)v[s].re - (double)f0.re;
-                    const double di = (double)v[s].im - (double)f0.im;
-                    s2 += (dr * dr + di * di) / (sk * sk);
-                    ndiff += (dr != 0.0 || di != 0.0) ? 1.0 : 0.0;
-                }
-                const double d2 = sqrt(block_sum<T>(s2, red) / N) / st.cdt;
-                const double nd = block_sum<T>(ndiff, red);
-                st.cdt = initdt_final(st.cdt, st.cz, d2, nd, dtmin, L);
+                st.cdt = fw ? init_after_f1<RF, LOGN, LOGE>(d.u0, (const CF*)d.kf[0], vf,
+                                                            d.abstol, d.reltol, st.cdt, st.cz, L,
+                                                            dtmin, red)
+                            : init_after_f1<RA, LOGN, LOGE>(d.lam[0], (const CA*)d.ka[0], va,
+                                                            st.abstol_adj, d.reltol, st.cdt,
+                                                            st.cz, L, dtmin, red);
             }
             st.stage = 0;
             if (fw) {
@@ -744,19 +801,20 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 st.naccept = st.nreject = st.iters = 0;
                 st.nf = 3;
                 if (d.ck_cap > 0) {
+                    const CF* k1 = (const CF*)d.kf[0];
 #pragma unroll
                     for (int s = 0; s < E; s++) {
-                        const int b = Sol::bin(s);
+                        const int b = SolF::bin(s);
                         reinterpret_cast<double2*>(d.ck_u)[b] =
                             reinterpret_cast<const double2*>(d.u0)[b];
-                        ((C*)d.ck_k1)[b] = k1[b];
+                        ((CF*)d.ck_k1)[b] = k1[b];
                     }
                 }
                 st.save_idx = 0;
                 while (st.save_idx < d.nsave && d.zsave[st.save_idx] == 0.0) {
                     double* o = d.save_out + (size_t)st.save_idx * 2 * N;
 #pragma unroll
-                    for (int s = 0; s < E; s++) st2(o, Sol::bin(s), ld2(d.u0, Sol::bin(s)));
+                    for (int s = 0; s < E; s++) st2(o, SolF::bin(s), ld2(d.u0, SolF::bin(s)));
                     st.save_idx++;
                 }
                 st.phase = PH_FWD;
@@ -774,9 +832,9 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 
         if (st.phase == PH_FWD || st.phase == PH_REC) {
             const bool rec = st.phase == PH_REC;
-            C* ko = Sol::kp(d.kf, st.kperm, st.stage);
+            CF* ko = SolF::kp(d.kf, st.kperm, st.stage);
 #pragma unroll
-            for (int s = 0; s < E; s++) ko[Sol::bin(s)] = v[s];
+            for (int s = 0; s < E; s++) ko[SolF::bin(s)] = vf[s];
             if (st.stage < 6) {
                 st.stage++;
                 continue;
@@ -786,14 +844,14 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double* u = d.u[st.cur];
             if (rec) {
                 // interpolant of this step: c0 = ũ_n, c_p = Σ_i r_ip k_i
-                C* sg = (C*)d.seg + (size_t)st.rec_pos * 5 * N;
+                CF* sg = (CF*)d.seg + (size_t)st.rec_pos * 5 * N;
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
-                    sg[b] = down<R>(ld2(u, b));
+                    const int b = SolF::bin(s);
+                    sg[b] = down<RF>(ld2(u, b));
                     double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
                     for (int i = 0; i < 7; i++) {
-                        const C ki = Sol::kp(d.kf, st.kperm, i)[b];
+                        const CF ki = SolF::kp(d.kf, st.kperm, i)[b];
 #pragma unroll
                         for (int q = 0; q < 4; q++) {
                             cr[q] += kT5r[i][q] * (double)ki.re;
@@ -801,7 +859,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                         }
                     }
 #pragma unroll
-                    for (int q = 0; q < 4; q++) sg[(q + 1) * N + b] = mk((R)cr[q], (R)ci[q]);
+                    for (int q = 0; q < 4; q++) sg[(q + 1) * N + b] = mk((RF)cr[q], (RF)ci[q]);
                 }
                 st.cur ^= 1;
                 st.kperm ^= 1;
@@ -811,7 +869,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
                 continue;
             }
-            const double EEst = S.error_norm(v, dt);
+            const double EEst = SF.error_norm(vf, dt);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;
                 st.phase = PH_DONE;
@@ -845,7 +903,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 double* o = d.save_out + (size_t)st.save_idx * 2 * N;
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
+                    const int b = SolF::bin(s);
                     double xr = 0.0, xi = 0.0;
                     for (int i = 0; i < 7; i++) {
                         double bi = 0.0, tp = th;
@@ -853,7 +911,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                             bi += kT5r[i][qq] * tp;
                             tp *= th;
                         }
-                        const C ki = Sol::kp(d.kf, st.kperm, i)[b];
+                        const CF ki = SolF::kp(d.kf, st.kperm, i)[b];
                         xr += bi * (double)ki.re;
                         xi += bi * (double)ki.im;
                     }
@@ -877,30 +935,31 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     for (int j = 1; j < d.ck_cap / 2; j++) {
 #pragma unroll
                         for (int s = 0; s < E; s++) {
-                            const int b = Sol::bin(s);
+                            const int b = SolF::bin(s);
                             reinterpret_cast<double2*>(d.ck_u)[(size_t)j * N + b] =
                                 reinterpret_cast<double2*>(d.ck_u)[(size_t)2 * j * N + b];
-                            ((C*)d.ck_k1)[(size_t)j * N + b] = ((C*)d.ck_k1)[(size_t)2 * j * N + b];
+                            ((CF*)d.ck_k1)[(size_t)j * N + b] =
+                                ((CF*)d.ck_k1)[(size_t)2 * j * N + b];
                         }
                     }
                     st.ck_stride *= 2;
                     slotc = st.nsteps / st.ck_stride;
                 }
                 const double* un = d.u[st.cur];
-                const C* k1 = Sol::kp(d.kf, st.kperm, 0);
+                const CF* k1 = SolF::kp(d.kf, st.kperm, 0);
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
+                    const int b = SolF::bin(s);
                     reinterpret_cast<double2*>(d.ck_u)[(size_t)slotc * N + b] =
                         reinterpret_cast<const double2*>(un)[b];
-                    ((C*)d.ck_k1)[(size_t)slotc * N + b] = k1[b];
+                    ((CF*)d.ck_k1)[(size_t)slotc * N + b] = k1[b];
                 }
             }
             if (st.z == L) {
                 const double* uf = d.u[st.cur];
 #pragma unroll
                 for (int s = 0; s < E; s++) {
-                    const int b = Sol::bin(s);
+                    const int b = SolF::bin(s);
                     const cx<double> x = ld2(uf, b);
                     const cx<double> p = phasor<double>(d.Dturns[b], L);
                     const cx<double> y = mk(x.re * p.re - x.im * p.im, x.re * p.im + x.im * p.re);
@@ -916,9 +975,9 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 
         // PH_ADJ
         {
-            C* ko = Sol::kp(d.ka, st.akperm, st.stage);
+            CA* ko = SolA::kp(d.ka, st.akperm, st.stage);
 #pragma unroll
-            for (int s = 0; s < E; s++) ko[Sol::bin(s)] = v[s];
+            for (int s = 0; s < E; s++) ko[SolF::bin(s)] = va[s];
             if (st.stage < 6) {
                 st.stage++;
                 continue;
@@ -926,7 +985,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             st.stage = 0;
             const double z = st.cz, dt = st.cdt;
             const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
-            const double EEst = S.error_norm(v, dt);
+            const double EEst = SA.error_norm(va, dt);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;
                 st.phase = PH_DONE;
@@ -956,7 +1015,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     st.phase = PH_FINAL;
                 } else {
                     st.seg--;
-                    restore_checkpoint<R, LOGN, LOGE>(d, st.seg, st);
+                    restore_checkpoint<RF, LOGN, LOGE>(d, st.seg, st);
                     st.phase = PH_REC;
                 }
             }

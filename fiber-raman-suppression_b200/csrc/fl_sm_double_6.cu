@@ -1,3 +1,3 @@
-// Single-mode stepper instance: double, Nt = 2^6, 2 elements per thread.
+// Single-mode stepper instance: FP64 throughout, Nt = 2^6, 2 elements per thread.
 #include "fl_sm_inst.cuh"
-FL_SM_INSTANCE(double, 6, 1)
+FL_SM_INSTANCE(double, double, double, 6, 1)

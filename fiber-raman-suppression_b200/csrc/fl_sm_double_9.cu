@@ -1,3 +1,3 @@
-// Single-mode stepper instance: double, Nt = 2^9, 16 elements per thread.
+// Single-mode stepper instance: FP64 throughout, Nt = 2^9, 16 elements per thread.
 #include "fl_sm_inst.cuh"
-FL_SM_INSTANCE(double, 9, 4)
+FL_SM_INSTANCE(double, double, double, 9, 4)

@@ -31,15 +31,16 @@ enum : int {
     ST_CAPACITY = 9
 };
 
-// Per-slot pointers and parameters.  R is float (FP32 mode) or double.
-// All field-sized buffers hold N complex values of the indicated type.
-template <typename R>
+// Per-slot pointers and parameters.  The forward solve and its recompute
+// run in precision RF (float in the default mode, double in the FP64 mode),
+// the adjoint in RA (double): typed buffers are void pointers whose element
+// type is stated beside them.  Field-sized buffers hold N values.
 struct SlotDesc {
-    // tables (shared by all slots of one fiber/grid)
+    // tables (shared by all slots of one fiber/grid); [0] float, [1] double
     const double* Dturns;   // D/(2 pi), turns per metre
-    const void* Heff;       // cx<R>: hR * (-1)^k  (fftshift folded in)
-    const void* ss;         // R: selfsteep = fftshift(ωs/ω0)
-    const void* tw;         // cx<R>: exp(-2 pi i k / N), k < N
+    const void* Heff[2];    // cx: hR * (-1)^k  (fftshift folded in)
+    const void* ss[2];      // real: selfsteep = fftshift(ωs/ω0)
+    const void* tw[2];      // cx: exp(-2 pi i k / N), k < N
     double gamma, one_m_fR;
     double L, reltol, abstol;
     int mode, log_cost;
@@ -58,17 +59,17 @@ struct SlotDesc {
     double* grad_out;       // N doubles (nullable)
     double* uL_out;         // N complex doubles: lab field at L (nullable)
     // workspace
-    double* u[2];           // FP64 states
+    double* u[2];           // FP64 forward states
     double* lam[2];         // FP64 adjoint states
-    void* kf[7];            // forward stages
-    void* ka[7];            // adjoint stages
-    void* scr[2];           // per-thread scratch fields
-    void* esv;              // error partial (cx<R>)
-    void* skv;              // error weights (R)
+    void* kf[7];            // forward stages, cx<RF>
+    void* ka[7];            // adjoint stages, cx<RA>
+    void* scr[2];           // per-thread scratch fields, cx<double>-sized
+    double* esv;            // error partial, N complex doubles
+    double* skv;            // error weights, N doubles
     double* ck_u;           // ck_cap * N complex doubles
-    void* ck_k1;            // ck_cap * N cx<R>
+    void* ck_k1;            // ck_cap * N cx<RF>
     double* steplog;        // 2 * step_cap doubles (z_n, dt_n)
-    void* seg;              // seg_cap * 5 * N cx<R>
+    void* seg;              // seg_cap * 5 * N cx<RF>: dense interpolant
 };
 
 struct SlotState {

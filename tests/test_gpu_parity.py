@@ -38,9 +38,10 @@ def test_rhs_matches_oracle(gpu_ctx, nt, precision):
     lam = (rng.standard_normal(fp.nt) + 1j * rng.standard_normal(fp.nt))[None, :] * 1e-3
     gp = GPUProblem(gpu_ctx, fp, precision)
     z = 0.3217
-    tol = 2e-6 if precision == "fp32" else 1e-12
+    # forward RHS in the mode's precision; the adjoint RHS is FP64 in both modes
+    tol = 2e-6 if precision == "fp32" else FIELD_TOL_FP64
     assert rel(gp.rhs(z, u), O.rhs_forward(fp, z, u)) < tol
-    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < tol
+    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < FIELD_TOL_FP64
 
 
 @pytest.mark.parametrize("nt,T", [(256, 3.0), (1024, 10.0), (2048, 10.0), (4096, 10.0)])
