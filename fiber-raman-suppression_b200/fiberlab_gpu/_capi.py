@@ -24,7 +24,8 @@ PRECISION = {"fp32": 0, "fp64": 1}
 EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_last_error", "fl_ctx_launch_count", "fl_ctx_synchronize", "fl_problem_create",
            "fl_problem_destroy", "fl_forward", "fl_adjoint", "fl_phase_gradient_batch",
-           "fl_phase_gradient_batch_device", "fl_rhs_eval", "fl_ctx_timing")
+           "fl_phase_gradient_batch_device", "fl_rhs_eval", "fl_ctx_timing",
+           "fl_forward_noalloc")
 
 
 class FlCtxOpts(C.Structure):
@@ -79,12 +80,26 @@ def load() -> C.CDLL:
         lib.fl_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_rhs_eval.argtypes = [vp, ip, dp, vp, vp, vp]
         lib.fl_ctx_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.fl_forward_noalloc.argtypes = [ip, ip, vp, dp, vp, vp, dp, dp, dp, dp, vp, vp, ip,
+                                           vp, vp, C.POINTER(FlStats)]
         _lib = lib
     return _lib
 
 
 def _ptr(a: np.ndarray) -> int:
     return a.ctypes.data
+
+
+def forward_noalloc(device: int, nt: int, d_D: int, gamma: float, d_hR: int, d_selfsteep: int,
+                    one_m_fR: float, L: float, reltol: float, abstol: float, d_u0: int,
+                    d_saveat: int, nsave: int, d_out: int, stream: int = 0):
+    """fl_forward_noalloc on caller-owned device buffers (integer device
+    addresses); returns (status, stats dict).  The call allocates nothing."""
+    st = FlStats()
+    rc = load().fl_forward_noalloc(device, nt, d_D, gamma, d_hR, d_selfsteep, one_m_fR, L,
+                                   reltol, abstol, d_u0, d_saveat, nsave, d_out, stream,
+                                   C.byref(st))
+    return rc, st.as_dict()
 
 
 class Context:

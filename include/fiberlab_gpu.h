@@ -153,6 +153,29 @@ int fl_phase_gradient_batch_device(fl_problem *prob, const double *d_u0, int nba
                                    int log_cost, double *d_J, double *d_grad,
                                    fl_stats *stats);
 
+/* Forward solve that allocates no device memory.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc -- host runtimes
+ * whose device memory is owned by their own pool allocator, and request loops
+ * that must not take cudaMalloc's implicit device synchronisation.  It runs
+ * the single-mode FP32 forward stepper on device buffers the caller owns:
+ *   d_D, d_selfsteep Nt doubles; d_hR Nt interleaved complex (the
+ *   fl_problem_create tables, M = 1); d_u0 Nt complex launch spectrum;
+ *   d_saveat nsave positions (sorted, first 0, last L); d_out_spectra
+ *   receives Nt*nsave complex lab-frame spectra; stream 0 = default stream.
+ * Everything else lives in one file-scope device array of 2 MiB that each GPU
+ * loading the library holds until the process exits.  Limit: Nt <= 2^13
+ * (larger grids return FL_EUNSUPPORTED) and 8192 accepted steps
+ * (FL_ECAPACITY).  The first call on a device resolves the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call reuses the same array, so calls that overlap on the
+ * GPU (other streams, other host threads) race; the state the solve needs
+ * is re-initialised by each call.  Invalid save positions or a non-finite or
+ * zero launch return FL_EINVAL. */
+int fl_forward_noalloc(int device, int nt, const double *d_D, double gamma, const double *d_hR,
+                       const double *d_selfsteep, double one_m_fR, double L, double reltol,
+                       double abstol, const double *d_u0, const double *d_saveat, int nsave,
+                       double *d_out_spectra, void *stream, fl_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif
