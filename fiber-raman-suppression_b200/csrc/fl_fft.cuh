@@ -142,6 +142,34 @@ struct FftShape {
     static constexpr int NPASS = NFULL + (REM > 0 ? 1 : 0);
 };
 
+// Twiddle factors W_N^e = exp(-2 pi i e / N), e in [0, N), from a two-level
+// table in shared memory: W^e = hi[e >> 6] * lo[e & 63] with both levels
+// copied from the correctly rounded full table (product error ~2 ulp).
+template <typename R, int LOGN>
+struct Twiddles {
+    static constexpr int N = 1 << LOGN;
+    static constexpr int NLO = N < 64 ? N : 64;
+    static constexpr int NHI = N / NLO;
+    static constexpr int SIZE = NLO + (NHI > 1 ? NHI : 0);  // entries in smem
+    const cx<R>* lo;
+    const cx<R>* hi;
+    __device__ __forceinline__ cx<R> operator()(int e) const {
+        if constexpr (NHI == 1) return lo[e];
+        else return cmul(hi[e >> 6], lo[e & 63]);
+    }
+    // fill from the full global table (all threads of the block; no sync)
+    __device__ static void fill(cx<R>* dst, const cx<R>* __restrict__ full) {
+        for (int i = threadIdx.x; i < SIZE; i += blockDim.x)
+            dst[i] = i < NLO ? full[i] : full[(i - NLO) * NLO];
+    }
+    __device__ static Twiddles at(const cx<R>* base) {
+        Twiddles t;
+        t.lo = base;
+        t.hi = base + NLO;
+        return t;
+    }
+};
+
 // The smem exchange moves whole complex values through one padded buffer,
 // or -- when that buffer would not fit in shared memory (FP64 at 2^14
 // points) -- the real and the imaginary parts in two rounds through a buffer
@@ -157,7 +185,7 @@ struct SmemPlan {
 // of the previous radices) on the E values of this thread.  The first pass
 // (ns = 1) has no twiddles.
 template <typename R, int LOGN, int LOGE, int RP, bool FIRST>
-__device__ __forceinline__ void pass_compute(cx<R> (&v)[1 << LOGE], const cx<R>* __restrict__ tw,
+__device__ __forceinline__ void pass_compute(cx<R> (&v)[1 << LOGE], const Twiddles<R, LOGN>& tw,
                                              const int ns) {
     using S = FftShape<LOGN, LOGE>;
     constexpr int E = S::E, T = S::T, N = S::N;
@@ -170,7 +198,7 @@ __device__ __forceinline__ void pass_compute(cx<R> (&v)[1 << LOGE], const cx<R>*
             const int m = (t + T * q) & (ns - 1);
             if constexpr (sizeof(R) == 8) {
                 // FP64: powers of one table twiddle (rounding stays ~1e-15)
-                const cx<R> w1 = tw[m * tws];
+                const cx<R> w1 = tw(m * tws);
                 cx<R> w = w1;
 #pragma unroll
                 for (int r = 1; r < RP; r++) {
@@ -180,7 +208,7 @@ __device__ __forceinline__ void pass_compute(cx<R> (&v)[1 << LOGE], const cx<R>*
             } else {
                 // FP32: every twiddle from the correctly rounded table
 #pragma unroll
-                for (int r = 1; r < RP; r++) v[q + BPT * r] = cmul(v[q + BPT * r], tw[m * r * tws]);
+                for (int r = 1; r < RP; r++) v[q + BPT * r] = cmul(v[q + BPT * r], tw(m * r * tws));
             }
         }
         dft_inreg<RP, false, BPT>(v, q);
@@ -270,7 +298,8 @@ __device__ __forceinline__ void gather_negated(const cx<R> (&v)[1 << LOGE], cx<R
 // the first and the last run as a runtime loop over one code body, so a
 // kernel carries one copy of each pass type.
 template <typename R, int LOGN, int LOGE>
-__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], void* sm, const cx<R>* tw) {
+__device__ __forceinline__ void block_fft(cx<R> (&v)[1 << LOGE], void* sm,
+                                          const Twiddles<R, LOGN>& tw) {
     using S = FftShape<LOGN, LOGE>;
     constexpr int E = S::E;
     constexpr int RL = S::REM ? (1 << S::REM) : E;  // radix of the last pass

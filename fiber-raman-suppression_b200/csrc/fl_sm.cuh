@@ -131,6 +131,28 @@ __device__ __forceinline__ double block_max(double v, double* red) {
     return s;
 }
 
+// Shared-memory layout of the stepper: [transform buffer][32 reduction
+// doubles][FP32 twiddles][FP64 twiddles].  red points at the reduction area.
+template <typename R, int LOGN>
+__device__ __forceinline__ const cx<R>* smem_twiddles(double* red) {
+    unsigned char* p = reinterpret_cast<unsigned char*>(red) + 32 * sizeof(double);
+    if constexpr (sizeof(R) == 8)
+        p += sizeof(cx<float>) * Twiddles<float, LOGN>::SIZE;
+    return reinterpret_cast<const cx<R>*>(p);
+}
+
+// Copy both precisions' twiddle tables into shared memory (the FP64 table is
+// absent when no adjoint will run) and wait for the block.
+template <int LOGN>
+__device__ __forceinline__ void load_twiddles(const SlotDesc& d, double* red) {
+    Twiddles<float, LOGN>::fill(const_cast<cx<float>*>(smem_twiddles<float, LOGN>(red)),
+                                (const cx<float>*)d.tw[0]);
+    if (d.tw[1])
+        Twiddles<double, LOGN>::fill(const_cast<cx<double>*>(smem_twiddles<double, LOGN>(red)),
+                                     (const cx<double>*)d.tw[1]);
+    __syncthreads();
+}
+
 // Block-level pieces of one problem's solve in RHS precision R.
 template <typename R, int LOGN, int LOGE>
 struct SmSolver {
@@ -142,15 +164,17 @@ struct SmSolver {
     const SlotDesc& d;
     void* sm;       // padded transform buffer
     double* red;    // 32 doubles
-    const C* tw;
-    const C* Heff;
-    const R* ss;
+    Twiddles<R, LOGN> tw;  // two-level table in shared memory
+    const C* __restrict__ Heff;
+    const R* __restrict__ ss;
+    const double* __restrict__ Dturns;
     C* scr0;
     C* scr1;
 
     __device__ SmSolver(const SlotDesc& dd, void* smem, double* r)
-        : d(dd), sm(smem), red(r), tw((const C*)dd.tw[P]), Heff((const C*)dd.Heff[P]),
-          ss((const R*)dd.ss[P]), scr0((C*)dd.scr[0]), scr1((C*)dd.scr[1]) {}
+        : d(dd), sm(smem), red(r), tw(Twiddles<R, LOGN>::at(smem_twiddles<R, LOGN>(r))),
+          Heff((const C*)dd.Heff[P]), ss((const R*)dd.ss[P]), Dturns(dd.Dturns),
+          scr0((C*)dd.scr[0]), scr1((C*)dd.scr[1]) {}
 
     __device__ __forceinline__ static int bin(int s) { return threadIdx.x + T * s; }
 
@@ -175,7 +199,7 @@ struct SmSolver {
             const int op = adj ? 8 + f : f;
             if (op == 0) {
 #pragma unroll
-                for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
+                for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(Dturns[bin(s)], z));
             } else if (op == 1) {
 #pragma unroll
                 for (int s = 0; s < E; s++) {
@@ -198,14 +222,14 @@ struct SmSolver {
 #pragma unroll
                 for (int s = 0; s < E; s++) {
                     const int b = bin(s);
-                    v[s] = scale(cmul(v[s], phasor<R>(d.Dturns[b], z)), ss[b]);
+                    v[s] = scale(cmul(v[s], phasor<R>(Dturns[b], z)), ss[b]);
                 }
             } else if (op == 9) {
 #pragma unroll
                 for (int s = 0; s < E; s++) scr0[bin(s)] = v[s];
                 load_u(v);
 #pragma unroll
-                for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(d.Dturns[bin(s)], z));
+                for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(Dturns[bin(s)], z));
             } else if (op == 10) {
 #pragma unroll
                 for (int s = 0; s < E; s++) {
@@ -250,7 +274,7 @@ struct SmSolver {
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int b = bin(s);
-            const C y = cmulc(v[s], phasor<R>(d.Dturns[b], z));  // e^{-iDz} x
+            const C y = cmulc(v[s], phasor<R>(Dturns[b], z));  // e^{-iDz} x
             const R sc = adj ? invn : ss[b] * invn;
             v[s] = mk(-y.im * sc, y.re * sc);                      // i y (τ) / N
         }
@@ -433,10 +457,13 @@ __device__ __noinline__ void rhs_adj_call(const SlotDesc* d, void* sm, double* r
     for (int s = 0; s < Sol::E; s++) vio[s] = v[s];
 }
 
-// transform buffer (sized for the adjoint precision) + 32 reduction doubles
+// transform buffer (sized for the adjoint precision), 32 reduction doubles
+// and the two twiddle tables
 template <typename RA, int LOGN>
 constexpr size_t smem_bytes() {
-    return SmemPlan<RA, LOGN>::BYTES + 32 * sizeof(double);
+    return SmemPlan<RA, LOGN>::BYTES + 32 * sizeof(double) +
+           sizeof(cx<float>) * Twiddles<float, LOGN>::SIZE +
+           sizeof(cx<double>) * Twiddles<double, LOGN>::SIZE;
 }
 
 // One RHS evaluation on one CTA (unit parity of the right-hand sides):
@@ -449,6 +476,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     using S = FftShape<LOGN, LOGE>;
     extern __shared__ __align__(16) unsigned char smraw[];
     double* red = reinterpret_cast<double*>(smraw + SmemPlan<RA, LOGN>::BYTES);
+    load_twiddles<LOGN>(*d, red);
     if (adjoint) {
         cx<RA> v[S::E];
 #pragma unroll
@@ -553,6 +581,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 
     const int slot = active[blockIdx.x];
     const SlotDesc& d = descs[slot];
+    load_twiddles<LOGN>(d, red);
     SlotState st = states[slot];  // block-uniform copy
     SolF SF(d, smraw, red);
     SolA SA(d, smraw, red);
