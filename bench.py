@@ -121,8 +121,9 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """dram bytes per stepper launch from the committed ncu summary, scaled to
-    the workload's batch by attempted steps (see profiles/)."""
+    """DRAM bytes per attempted (forward or adjoint) step from the committed
+    ncu capture of the stepper (profiles/sm_advance_traffic.json); the bench
+    scales it to its own launch by the attempted steps of that launch."""
     p = os.path.join(ROOT, "profiles", "sm_advance_traffic.json")
     if os.path.exists(p):
         with open(p) as f:
@@ -246,7 +247,7 @@ def run_ours(args):
     tr = profiled_traffic()
     traffic = None
     if tr and tr.get("bytes_per_attempted_step"):
-        traffic = tr["bytes_per_attempted_step"] * (fwd_att + rec + adj_att)
+        traffic = tr["bytes_per_attempted_step"] * (fwd_att + adj_att)
 
     # end to end through the public host API (host buffers, copies inside)
     e2e_t = []
