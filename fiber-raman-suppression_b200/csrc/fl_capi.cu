@@ -15,6 +15,7 @@
 
 #include "../../include/fiberlab_gpu.h"
 #include "fl_launch.h"
+#include "fl_mm_launch.h"
 
 using namespace fl;
 
@@ -97,9 +98,12 @@ bool gamma_symmetric(const double* g, int m) {
     return true;
 }
 
+// u_shaped = u0 ⊙ cis(φ_b) (physics_models.jl:791-797): one phase per time
+// bin shared by the modes, or (per_mode) one per (t, m)
 __global__ void shaped_launch_kernel(const double2* __restrict__ u0,
                                      const double* __restrict__ phases, int nt, int m,
-                                     int nbatch, double2* __restrict__ out, size_t out_stride) {
+                                     int nbatch, double2* __restrict__ out, size_t out_stride,
+                                     int per_mode = 0) {
     const long total = (long)nt * m * nbatch;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total;
          i += (long)gridDim.x * blockDim.x) {
@@ -107,7 +111,7 @@ __global__ void shaped_launch_kernel(const double2* __restrict__ u0,
         const long q = i % ((long)nt * m);
         const int t = (int)(q % nt);
         double s, c;
-        sincos(phases[(long)b * nt + t], &s, &c);
+        sincos(per_mode ? phases[(long)b * nt * m + q] : phases[(long)b * nt + t], &s, &c);
         const double2 x = u0[q];
         out[(size_t)b * out_stride + q] = make_double2(x.x * c - x.y * s, x.x * s + x.y * c);
     }
@@ -130,8 +134,10 @@ struct fl_problem {
     void* d_Heff[2] = {nullptr, nullptr};  // [0] float, [1] double
     void* d_ss[2] = {nullptr, nullptr};
     void* d_tw[2] = {nullptr, nullptr};
+    void* d_G[2] = {nullptr, nullptr};     // multimode contraction matrix [0] float, [1] double
     // workspace of the last forward (kept for fl_adjoint)
     struct Work* last = nullptr;
+    struct MmWork* mlast = nullptr;        // same for multimode problems
 };
 
 // Per-batch workspace: one allocation carved into per-slot buffers.
@@ -326,9 +332,6 @@ void fill_stats(const SlotState& s, fl_stats* o) {
 
 int check_problem(fl_problem* pr) {
     if (!pr || !pr->ctx) return FL_EINVAL;
-    if (pr->m != 1)
-        return set_err(pr->ctx, FL_EUNSUPPORTED,
-                       "multimode problems (M=%d) go through the multimode stepper", pr->m);
     return FL_OK;
 }
 
@@ -389,6 +392,414 @@ int set_mode(fl_ctx* ctx, Work* w, int mode, int log_cost) {
     }
     CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), w->h_desc.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
+    return FL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// multimode (M > 1) runtime
+// ---------------------------------------------------------------------------
+
+}  // namespace
+
+// Per-batch multimode workspace, carved like Work.
+struct MmWork {
+    fl_ctx* ctx = nullptr;
+    int B = 0, nt = 0, m = 0, np = 0, K = 0, segcap = 0, stepcap = 0, nsave = 0;
+    int per_mode = 0;
+    char* pool = nullptr;
+    size_t pool_bytes = 0;
+    void* d_desc = nullptr;
+    MmState* d_state = nullptr;
+    int* d_active = nullptr;
+    int* d_ndone = nullptr;
+    int* h_ndone = nullptr;          // pinned
+    std::vector<MmDesc> h_desc;
+    double* d_u0 = nullptr;          // B * NM complex
+    double* d_save = nullptr;        // B * nsave * NM complex
+    double* d_lamL = nullptr;
+    double* d_lam0 = nullptr;
+    double* d_grad = nullptr;        // B * NM
+    double* d_uL = nullptr;
+    double* d_zsave = nullptr;
+    unsigned char* d_mask = nullptr;
+
+    ~MmWork() {
+        cudaFree(pool);
+        cudaFree(d_desc);
+        cudaFree(d_state);
+        cudaFree(d_active);
+        cudaFree(d_ndone);
+        cudaFreeHost(h_ndone);
+    }
+};
+
+namespace {
+
+size_t mm_slot_bytes(size_t nm, size_t npn, size_t rf, int K, int segcap, int stepcap, int M) {
+    const size_t C = 2 * rf * nm, D2 = 16 * nm;
+    size_t b = 0;
+    b += 4 * D2;                         // u[2], lam[2]
+    b += 7 * C + 7 * D2;                 // kf, ka
+    b += 2 * D2 + 8 * nm + 8 * (size_t)M;  // probe, esv, skv, part
+    b += (size_t)K * (D2 + C);           // checkpoints
+    b += 16 * (size_t)stepcap;           // step log
+    b += (size_t)segcap * 5 * C;         // recompute segment
+    b += 3 * D2 + 2 * 8 * npn;           // ut, lt, eta, sq, cq
+    return b + 40 * 256;                 // alignment of the carved buffers
+}
+
+int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmWork** out) {
+    fl_ctx* ctx = pr->ctx;
+    const size_t rf = pr->precision == FL_PRECISION_FP64 ? 8 : 4;
+    auto w = std::make_unique<MmWork>();
+    w->ctx = ctx;
+    w->B = B;
+    w->nt = pr->nt;
+    w->m = pr->m;
+    w->np = pr->m * (pr->m + 1) / 2;
+    w->K = ctx->opts.checkpoints;
+    w->segcap = ctx->opts.segment_steps;
+    w->stepcap = ctx->opts.step_log;
+    w->nsave = nsave;
+    w->per_mode = per_mode;
+    const size_t nm = (size_t)pr->nt * pr->m, npn = (size_t)w->np * pr->nt;
+    const size_t per = mm_slot_bytes(nm, npn, rf, w->K, w->segcap, w->stepcap, pr->m);
+    const size_t io = 16 * nm * (4 + nsave) + 8 * nm + 256 * 8;
+    w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + pr->nt + 4096;
+    if (ctx->opts.hbm_budget_bytes && w->pool_bytes > ctx->opts.hbm_budget_bytes)
+        return set_err(ctx, FL_OOM_ADMISSION, "workspace of %zu bytes exceeds the HBM budget",
+                       w->pool_bytes);
+    CU(cudaMalloc(&w->pool, w->pool_bytes));
+    CU(cudaMalloc(&w->d_desc, sizeof(MmDesc) * B));
+    CU(cudaMalloc(&w->d_state, sizeof(MmState) * B));
+    CU(cudaMalloc(&w->d_active, sizeof(int) * B));
+    CU(cudaMalloc(&w->d_ndone, sizeof(int)));
+    CU(cudaMallocHost(&w->h_ndone, sizeof(int)));
+    char* p = w->pool;
+    w->d_zsave = (double*)carve(p, 8 * (size_t)std::max(nsave, 1));
+    w->d_mask = (unsigned char*)carve(p, pr->nt);
+    w->d_u0 = (double*)carve(p, 16 * nm * B);
+    w->d_lamL = (double*)carve(p, 16 * nm * B);
+    w->d_lam0 = (double*)carve(p, 16 * nm * B);
+    w->d_uL = (double*)carve(p, 16 * nm * B);
+    w->d_grad = (double*)carve(p, 8 * nm * B);
+    w->d_save = nsave ? (double*)carve(p, 16 * nm * nsave * B) : nullptr;
+    w->h_desc.assign(B, MmDesc{});
+    const size_t C = 2 * rf * nm, D2 = 16 * nm;
+    for (int b = 0; b < B; b++) {
+        MmDesc& d = w->h_desc[b];
+        d.Dturns = pr->d_Dturns;
+        for (int q = 0; q < 2; q++) {
+            d.Heff[q] = pr->d_Heff[q];
+            d.ss[q] = pr->d_ss[q];
+            d.tw[q] = pr->d_tw[q];
+            d.G[q] = pr->d_G[q];
+        }
+        d.M = pr->m;
+        d.NP = w->np;
+        d.N = pr->nt;
+        d.fp64 = pr->precision == FL_PRECISION_FP64;
+        d.one_m_fR = pr->one_m_fR;
+        d.L = pr->L;
+        d.reltol = pr->reltol;
+        d.abstol = pr->abstol;
+        d.mode = mode;
+        d.log_cost = 0;
+        d.nsave = nsave;
+        d.phase_per_mode = per_mode;
+        d.ck_cap = w->K;
+        d.seg_cap = w->segcap;
+        d.step_cap = w->stepcap;
+        d.max_iters = ctx->opts.max_iters;
+        d.zsave = w->d_zsave;
+        d.save_out = nsave ? w->d_save + (size_t)b * 2 * nm * nsave : nullptr;
+        d.u0 = w->d_u0 + (size_t)b * 2 * nm;
+        d.mask = w->d_mask;
+        d.lamL = w->d_lamL + (size_t)b * 2 * nm;
+        d.lam0_out = w->d_lam0 + (size_t)b * 2 * nm;
+        d.grad_out = w->d_grad + (size_t)b * nm;
+        d.uL_out = w->d_uL + (size_t)b * 2 * nm;
+        for (int i = 0; i < 2; i++) d.u[i] = (double*)carve(p, D2);
+        for (int i = 0; i < 2; i++) d.lam[i] = (double*)carve(p, D2);
+        for (int i = 0; i < 7; i++) d.kf[i] = carve(p, C);
+        for (int i = 0; i < 7; i++) d.ka[i] = carve(p, D2);
+        d.probe = carve(p, D2);
+        d.esv = (double*)carve(p, D2);
+        d.skv = (double*)carve(p, 8 * nm);
+        d.part = (double*)carve(p, 8 * (size_t)pr->m);
+        d.ck_u = (double*)carve(p, D2 * w->K);
+        d.ck_k1 = carve(p, C * w->K);
+        d.steplog = (double*)carve(p, 16 * (size_t)w->stepcap);
+        d.seg = carve(p, C * 5 * (size_t)w->segcap);
+        d.ut = carve(p, D2);
+        d.lt = carve(p, D2);
+        d.eta = carve(p, D2);
+        d.sq = carve(p, 8 * npn);
+        d.cq = carve(p, 8 * npn);
+    }
+    if ((size_t)(p - w->pool) > w->pool_bytes)
+        return set_err(ctx, FL_ECUDA, "internal: workspace overflow (%zu > %zu)",
+                       (size_t)(p - w->pool), w->pool_bytes);
+    CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), sizeof(MmDesc) * B, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    std::vector<int> act(B);
+    for (int b = 0; b < B; b++) act[b] = b;
+    CU(cudaMemcpyAsync(w->d_active, act.data(), sizeof(int) * B, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaMemsetAsync(w->d_state, 0, sizeof(MmState) * B, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    *out = w.release();
+    return FL_OK;
+}
+
+int mm_set_mode(fl_ctx* ctx, MmWork* w, int mode, int log_cost) {
+    for (auto& d : w->h_desc) {
+        d.mode = mode;
+        d.log_cost = log_cost;
+    }
+    CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), sizeof(MmDesc) * w->B, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    return FL_OK;
+}
+
+MmRound mm_round_args(fl_problem* pr, MmWork* w, int nactive) {
+    MmRound a{};
+    a.desc = w->d_desc;
+    a.state = w->d_state;
+    a.active = w->d_active;
+    a.nactive = nactive;
+    a.M = pr->m;
+    a.NP = w->np;
+    a.N = pr->nt;
+    a.fp64 = pr->precision == FL_PRECISION_FP64;
+    a.control = 1;
+    a.ndone = nullptr;
+    a.stream = pr->ctx->stream;
+    return a;
+}
+
+// Evaluation rounds until every one of the first nactive slots is done: one
+// control pass prepares each slot's first evaluation, then batches of rounds
+// run with the finished-slot count read back after each batch.  Every slot
+// has its own attempted-step limits, so the loop ends; the host bound below
+// only guards against a control bug.
+int mm_run(fl_problem* pr, MmWork* w, int nactive) {
+    fl_ctx* ctx = pr->ctx;
+    MmRoundFn round = mm_round_launcher(ilog2i(pr->nt));
+    if (!round) return set_err(ctx, FL_EUNSUPPORTED, "multimode Nt = %d is not built", pr->nt);
+    MmRound a = mm_round_args(pr, w, nactive);
+    CU(cudaEventRecord(ctx->ev[2], ctx->stream));
+    CU(mm_launch_control(a, 0));
+    ctx->launches++;
+    const int per_batch = 8;
+    const long max_rounds = 4 * 7 * (ctx->opts.max_iters + 2) + 64;
+    long rounds = 0;
+    for (;;) {
+        for (int r = 0; r < per_batch; r++) {
+            a.ndone = nullptr;
+            if (r == per_batch - 1) {
+                CU(cudaMemsetAsync(w->d_ndone, 0, sizeof(int), ctx->stream));
+                a.ndone = w->d_ndone;
+            }
+            CU(round(a));
+            ctx->launches += a.fp64 ? 7 : 10;
+        }
+        rounds += per_batch;
+        CU(cudaMemcpyAsync(w->h_ndone, w->d_ndone, sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CU(cudaStreamSynchronize(ctx->stream));
+        if (*w->h_ndone >= nactive) break;
+        if (rounds > max_rounds)
+            return set_err(ctx, FL_MAXITERS, "multimode stepper did not finish in %ld rounds",
+                           rounds);
+    }
+    CU(cudaEventRecord(ctx->ev[3], ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+    ctx->kernel_ms = ms;
+    return FL_OK;
+}
+
+int mm_read_states(fl_ctx* ctx, MmWork* w, int n, std::vector<MmState>& st) {
+    st.resize(n);
+    CU(cudaMemcpyAsync(st.data(), w->d_state, sizeof(MmState) * n, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
+void mm_fill_stats(const MmState& s, fl_stats* o) {
+    o->naccept = s.naccept;
+    o->nreject = s.nreject;
+    o->nf = s.nf;
+    o->adj_naccept = s.a_naccept;
+    o->adj_nreject = s.a_nreject;
+    o->adj_nf = s.a_nf;
+    o->status = s.status;
+    o->checkpoints_used = s.ck_stride > 0 ? (s.nsteps + s.ck_stride - 1) / s.ck_stride : 0;
+    o->J = s.J;
+    o->z_end = s.z;
+}
+
+__global__ void mm_gather_J_kernel(const MmState* __restrict__ st, int n, double* __restrict__ J) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) J[i] = st[i].J;
+}
+
+// G[(i*M + j)*NP + q] = γ[i,j,k,l] + γ[i,j,l,k] (k < l), γ[i,j,k,k] (k = l),
+// q enumerating k <= l row by row; γ in the reference's column-major order
+int mm_upload_G(fl_problem* pr, const double* gamma) {
+    fl_ctx* ctx = pr->ctx;
+    const int M = pr->m, NP = M * (M + 1) / 2;
+    auto g = [&](int i, int j, int k, int l) { return gamma[i + M * (j + M * (k + M * l))]; };
+    std::vector<double> G((size_t)M * M * NP);
+    std::vector<float> Gf(G.size());
+    for (int i = 0; i < M; i++)
+        for (int j = 0; j < M; j++) {
+            int q = 0;
+            for (int k = 0; k < M; k++)
+                for (int l = k; l < M; l++, q++) {
+                    const double v = k == l ? g(i, j, k, k) : g(i, j, k, l) + g(i, j, l, k);
+                    G[((size_t)i * M + j) * NP + q] = v;
+                    Gf[((size_t)i * M + j) * NP + q] = (float)v;
+                }
+        }
+    CU(cudaMalloc(&pr->d_G[0], sizeof(float) * Gf.size()));
+    CU(cudaMalloc(&pr->d_G[1], sizeof(double) * G.size()));
+    CU(cudaMemcpy(pr->d_G[0], Gf.data(), sizeof(float) * Gf.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_G[1], G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice));
+    return FL_OK;
+}
+
+int mm_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave,
+               double* out_spectra, fl_stats* stats) {
+    fl_ctx* ctx = pr->ctx;
+    const size_t nm = (size_t)pr->nt * pr->m;
+    delete pr->mlast;
+    pr->mlast = nullptr;
+    MmWork* w = nullptr;
+    int rc = mm_work_create(pr, 1, nsave, MODE_FORWARD, 0, &w);
+    if (rc) return rc;
+    pr->mlast = w;
+    CU(cudaMemcpyAsync(w->d_u0, u0, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
+    if (nsave)
+        CU(cudaMemcpyAsync(w->d_zsave, saveat, 8 * (size_t)nsave, cudaMemcpyHostToDevice,
+                           ctx->stream));
+    rc = mm_run(pr, w, 1);
+    if (rc) return rc;
+    std::vector<MmState> st;
+    rc = mm_read_states(ctx, w, 1, st);
+    if (rc) return rc;
+    if (stats) mm_fill_stats(st[0], stats);
+    if (st[0].status) return set_err(ctx, st[0].status, "%s", fl_status_string(st[0].status));
+    if (nsave) CU(cudaMemcpy(out_spectra, w->d_save, 16 * nm * nsave, cudaMemcpyDeviceToHost));
+    return FL_OK;
+}
+
+int mm_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats* stats) {
+    fl_ctx* ctx = pr->ctx;
+    const size_t nm = (size_t)pr->nt * pr->m;
+    MmWork* w = pr->mlast;
+    std::vector<MmState> st;
+    int rc = mm_read_states(ctx, w, 1, st);
+    if (rc) return rc;
+    if (st[0].phase != PH_DONE || st[0].status != ST_OK)
+        return set_err(ctx, FL_EINVAL, "the last forward did not complete");
+    st[0].phase = PH_SEED;
+    CU(cudaMemcpyAsync(w->d_state, st.data(), sizeof(MmState), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    rc = mm_set_mode(ctx, w, MODE_SEEDED_ADJOINT, 0);
+    if (rc) return rc;
+    CU(cudaMemcpyAsync(w->d_lamL, lambdaL, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
+    rc = mm_run(pr, w, 1);
+    if (rc) return rc;
+    rc = mm_read_states(ctx, w, 1, st);
+    if (rc) return rc;
+    if (stats) mm_fill_stats(st[0], stats);
+    if (st[0].status) return set_err(ctx, st[0].status, "%s", fl_status_string(st[0].status));
+    CU(cudaMemcpy(lambda0, w->d_lam0, 16 * nm, cudaMemcpyDeviceToHost));
+    return FL_OK;
+}
+
+// one RHS evaluation through the multimode kernels (no control pass)
+int mm_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const double* u_fwd,
+                double* du_out) {
+    fl_ctx* ctx = pr->ctx;
+    const size_t nm = (size_t)pr->nt * pr->m;
+    MmRoundFn round = mm_round_launcher(ilog2i(pr->nt));
+    if (!round) return set_err(ctx, FL_EUNSUPPORTED, "multimode Nt = %d is not built", pr->nt);
+    MmWork* w = nullptr;
+    int rc = mm_work_create(pr, 1, 0, MODE_FORWARD, 0, &w);
+    if (rc) return rc;
+    std::unique_ptr<MmWork> hold(w);
+    CU(cudaMemcpyAsync(w->d_u0, u_in, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
+    if (adjoint) CU(cudaMemcpyAsync(w->d_lamL, u_fwd, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
+    MmState st{};
+    st.phase = adjoint ? PH_EVAL_ADJ : PH_EVAL_FWD;
+    st.ez = st.ezload = z;
+    CU(cudaMemcpyAsync(w->d_state, &st, sizeof st, cudaMemcpyHostToDevice, ctx->stream));
+    MmRound a = mm_round_args(pr, w, 1);
+    a.control = 0;
+    CU(round(a));
+    ctx->launches += a.fp64 ? 6 : 9;
+    CU(cudaMemcpyAsync(du_out, w->d_lam0, 16 * nm, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
+// batched forward + band objective + adjoint + phase gradient of the
+// multimode stepper on device buffers; phases (Nt, B) shared by the modes or
+// (Nt, M, B) per mode; grad has the shape of the phases
+int mm_phase_gradient_device(fl_problem* pr, const double* d_u0, int nbatch,
+                             const double* d_phases, int per_mode, const unsigned char* d_mask,
+                             int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+    fl_ctx* ctx = pr->ctx;
+    const int nt = pr->nt;
+    const size_t nm = (size_t)nt * pr->m;
+    if (!pr->mlast || pr->mlast->B < nbatch || pr->mlast->nsave != 0 ||
+        pr->mlast->per_mode != per_mode) {
+        delete pr->mlast;
+        pr->mlast = nullptr;
+        MmWork* w = nullptr;
+        int rc = mm_work_create(pr, nbatch, 0, MODE_BAND_GRADIENT, per_mode, &w);
+        if (rc) return rc;
+        pr->mlast = w;
+    }
+    MmWork* w = pr->mlast;
+    CU(cudaEventRecord(ctx->ev[0], ctx->stream));
+    int rc = mm_set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost);
+    if (rc) return rc;
+    CU(cudaMemsetAsync(w->d_state, 0, sizeof(MmState) * nbatch, ctx->stream));
+    CU(cudaMemcpyAsync(w->d_mask, d_mask, nt, cudaMemcpyDeviceToDevice, ctx->stream));
+    const int threads = 256;
+    const long total = (long)nm * nbatch;
+    const int blocks = (int)std::min<long>((total + threads - 1) / threads, 4096);
+    shaped_launch_kernel<<<blocks, threads, 0, ctx->stream>>>(
+        (const double2*)d_u0, d_phases, nt, pr->m, nbatch, (double2*)w->d_u0, nm, per_mode);
+    ctx->launches++;
+    CU(cudaGetLastError());
+    rc = mm_run(pr, w, nbatch);
+    if (rc) return rc;
+    mm_gather_J_kernel<<<(nbatch + 255) / 256, 256, 0, ctx->stream>>>(w->d_state, nbatch, d_J);
+    ctx->launches++;
+    CU(cudaGetLastError());
+    // per-slot gradients are NM apart; the caller's are N (shared) or NM (per mode) apart
+    const size_t gl = per_mode ? nm : (size_t)nt;
+    CU(cudaMemcpy2DAsync(d_grad, 8 * gl, w->d_grad, 8 * nm, 8 * gl, nbatch,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaEventRecord(ctx->ev[1], ctx->stream));
+    std::vector<MmState> st;
+    rc = mm_read_states(ctx, w, nbatch, st);
+    if (rc) return rc;
+    float ms = 0.f;
+    CU(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    ctx->call_ms = ms;
+    if (stats)
+        for (int b = 0; b < nbatch; b++) mm_fill_stats(st[b], &stats[b]);
+    for (int b = 0; b < nbatch; b++)
+        if (st[b].status != ST_OK)
+            return set_err(ctx, st[b].status, "slot %d: %s", b, fl_status_string(st[b].status));
     return FL_OK;
 }
 
@@ -530,8 +941,12 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
     pr->abstol = abstol;
     pr->gamma0 = gamma[0];
     pr->gamma_sym = gamma_symmetric(gamma, m);
+    if (m > 1 && (!mm_supported_modes(m) || !mm_round_launcher(ilog2i(nt))))
+        return set_err(ctx, FL_EUNSUPPORTED, "multimode problems are built for M = 2..10 and "
+                       "Nt = 2^6..2^14 (got M = %d, Nt = %d)", m, nt);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
     int rc = upload_tables(pr.get(), D, hR, selfsteep);
+    if (!rc && m > 1) rc = mm_upload_G(pr.get(), gamma);
     if (rc) {
         fl_problem_destroy(pr.release());
         return rc;
@@ -543,6 +958,9 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
 int fl_problem_destroy(fl_problem* pr) {
     if (!pr) return FL_EINVAL;
     delete pr->last;
+    delete pr->mlast;
+    cudaFree(pr->d_G[0]);
+    cudaFree(pr->d_G[1]);
     cudaFree(pr->d_Dturns);
     for (int q = 0; q < 2; q++) {
         cudaFree(pr->d_Heff[q]);
@@ -579,6 +997,7 @@ int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave
     }
     if (!(nrm > 0)) return set_err(ctx, FL_EINVAL, "input spectrum must be nonzero");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    if (pr->m > 1) return mm_forward(pr, u0, saveat, nsave, out_spectra, stats);
     delete pr->last;
     pr->last = nullptr;
     Work* w = nullptr;
@@ -609,11 +1028,14 @@ int fl_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats*
     if (!pr->gamma_sym)
         return set_err(ctx, FL_NONSYMMETRIC,
                        "fiber adjoint requires a fully permutation-symmetric gamma tensor");
-    if (!pr->last) return set_err(ctx, FL_EINVAL, "fl_adjoint needs a preceding fl_forward");
+    if (!(pr->m > 1 ? (void*)pr->mlast : (void*)pr->last))
+        return set_err(ctx, FL_EINVAL, "fl_adjoint needs a preceding fl_forward");
     const int nt = pr->nt;
     for (int i = 0; i < 2 * nt * pr->m; i++)
         if (!std::isfinite(lambdaL[i]))
             return set_err(ctx, FL_EINVAL, "adjoint terminal condition must be finite");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    if (pr->m > 1) return mm_adjoint(pr, lambdaL, lambda0, stats);
     Work* w = pr->last;
     std::vector<SlotState> st;
     rc = read_states(ctx, w, st);
@@ -647,6 +1069,7 @@ int fl_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const
         return set_err(ctx, FL_NONSYMMETRIC,
                        "fiber adjoint requires a fully permutation-symmetric gamma tensor");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    if (pr->m > 1) return mm_rhs_eval(pr, adjoint, z, u_in, u_fwd, du_out);
     const int fp64 = pr->precision == FL_PRECISION_FP64;
     RhsFn fn = rhs_launcher(fp64, ilog2i(pr->nt));
     if (!fn) return set_err(ctx, FL_EUNSUPPORTED, "Nt = %d is not built", pr->nt);
@@ -703,9 +1126,10 @@ static int phase_gradient_core(fl_problem* pr, Work* w, int nbatch, const double
     return status_of_slots(ctx, st);
 }
 
-int fl_phase_gradient_batch_device(fl_problem* pr, const double* d_u0, int nbatch,
-                                   const double* d_phases, const unsigned char* d_mask,
-                                   int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+static int phase_gradient_device(fl_problem* pr, const double* d_u0, int nbatch,
+                                 const double* d_phases, int per_mode,
+                                 const unsigned char* d_mask, int log_cost, double* d_J,
+                                 double* d_grad, fl_stats* stats) {
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
@@ -715,6 +1139,10 @@ int fl_phase_gradient_batch_device(fl_problem* pr, const double* d_u0, int nbatc
         return set_err(ctx, FL_NONSYMMETRIC,
                        "fiber adjoint requires a fully permutation-symmetric gamma tensor");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    if (pr->m > 1)
+        return mm_phase_gradient_device(pr, d_u0, nbatch, d_phases, per_mode, d_mask, log_cost,
+                                        d_J, d_grad, stats);
+    // single mode: a per-mode phase is the shared phase
     // keep one workspace per problem sized for the largest batch seen
     if (!pr->last || pr->last->B < nbatch || pr->last->nsave != 0) {
         delete pr->last;
@@ -738,35 +1166,38 @@ int fl_phase_gradient_batch_device(fl_problem* pr, const double* d_u0, int nbatc
                                stats);
 }
 
-int fl_phase_gradient_batch(fl_problem* pr, const double* u0, int nbatch, const double* phases,
-                            const unsigned char* mask, int log_cost, double* J, double* grad,
-                            fl_stats* stats) {
+// host-buffer form: copies in, runs the device form, copies out
+static int phase_gradient_host(fl_problem* pr, const double* u0, int nbatch,
+                               const double* phases, int per_mode, const unsigned char* mask,
+                               int log_cost, double* J, double* grad, fl_stats* stats) {
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
     if (!u0 || !phases || !mask || !J || !grad || nbatch < 1)
         return set_err(ctx, FL_EINVAL, "null argument");
     const int nt = pr->nt;
+    const size_t nm = (size_t)nt * pr->m;
+    const size_t np = (per_mode ? nm : (size_t)nt) * nbatch;  // phase (and gradient) values
     bool any = false;
     for (int i = 0; i < nt; i++) any |= mask[i] != 0;
     if (!any) return set_err(ctx, FL_EINVAL, "band mask must contain at least one bin");
-    for (long i = 0; i < (long)nt * nbatch; i++)
+    for (size_t i = 0; i < np; i++)
         if (!std::isfinite(phases[i])) return set_err(ctx, FL_EINVAL, "phase values must be finite");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
     double *d_u0 = nullptr, *d_ph = nullptr, *d_J = nullptr, *d_g = nullptr;
     unsigned char* d_m = nullptr;
-    CU(cudaMallocAsync(&d_u0, 16 * (size_t)nt, ctx->stream));
-    CU(cudaMallocAsync(&d_ph, 8 * (size_t)nt * nbatch, ctx->stream));
+    CU(cudaMallocAsync(&d_u0, 16 * nm, ctx->stream));
+    CU(cudaMallocAsync(&d_ph, 8 * np, ctx->stream));
     CU(cudaMallocAsync(&d_J, 8 * (size_t)nbatch, ctx->stream));
-    CU(cudaMallocAsync(&d_g, 8 * (size_t)nt * nbatch, ctx->stream));
+    CU(cudaMallocAsync(&d_g, 8 * np, ctx->stream));
     CU(cudaMallocAsync(&d_m, nt, ctx->stream));
-    CU(cudaMemcpyAsync(d_u0, u0, 16 * (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
-    CU(cudaMemcpyAsync(d_ph, phases, 8 * (size_t)nt * nbatch, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(d_u0, u0, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(d_ph, phases, 8 * np, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(d_m, mask, nt, cudaMemcpyHostToDevice, ctx->stream));
-    rc = fl_phase_gradient_batch_device(pr, d_u0, nbatch, d_ph, d_m, log_cost, d_J, d_g, stats);
+    rc = phase_gradient_device(pr, d_u0, nbatch, d_ph, per_mode, d_m, log_cost, d_J, d_g, stats);
     if (rc == FL_OK) {
         CU(cudaMemcpyAsync(J, d_J, 8 * (size_t)nbatch, cudaMemcpyDeviceToHost, ctx->stream));
-        CU(cudaMemcpyAsync(grad, d_g, 8 * (size_t)nt * nbatch, cudaMemcpyDeviceToHost, ctx->stream));
+        CU(cudaMemcpyAsync(grad, d_g, 8 * np, cudaMemcpyDeviceToHost, ctx->stream));
     }
     cudaFreeAsync(d_u0, ctx->stream);
     cudaFreeAsync(d_ph, ctx->stream);
@@ -775,6 +1206,37 @@ int fl_phase_gradient_batch(fl_problem* pr, const double* u0, int nbatch, const 
     cudaFreeAsync(d_m, ctx->stream);
     CU(cudaStreamSynchronize(ctx->stream));
     return rc;
+}
+
+int fl_phase_gradient_batch_device(fl_problem* pr, const double* d_u0, int nbatch,
+                                   const double* d_phases, const unsigned char* d_mask,
+                                   int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+    return phase_gradient_device(pr, d_u0, nbatch, d_phases, 0, d_mask, log_cost, d_J, d_grad,
+                                 stats);
+}
+
+int fl_phase_gradient_batch(fl_problem* pr, const double* u0, int nbatch, const double* phases,
+                            const unsigned char* mask, int log_cost, double* J, double* grad,
+                            fl_stats* stats) {
+    return phase_gradient_host(pr, u0, nbatch, phases, 0, mask, log_cost, J, grad, stats);
+}
+
+int fl_mode_phase_gradient_batch_device(fl_problem* pr, const double* d_u0, int nbatch,
+                                        const double* d_phases, const unsigned char* d_mask,
+                                        int log_cost, double* d_J, double* d_grad,
+                                        fl_stats* stats) {
+    if (pr && pr->m == 1)
+        return phase_gradient_device(pr, d_u0, nbatch, d_phases, 0, d_mask, log_cost, d_J,
+                                     d_grad, stats);
+    return phase_gradient_device(pr, d_u0, nbatch, d_phases, 1, d_mask, log_cost, d_J, d_grad,
+                                 stats);
+}
+
+int fl_mode_phase_gradient_batch(fl_problem* pr, const double* u0, int nbatch,
+                                 const double* phases, const unsigned char* mask, int log_cost,
+                                 double* J, double* grad, fl_stats* stats) {
+    return phase_gradient_host(pr, u0, nbatch, phases, pr && pr->m > 1 ? 1 : 0, mask, log_cost,
+                               J, grad, stats);
 }
 
 }  // extern "C"

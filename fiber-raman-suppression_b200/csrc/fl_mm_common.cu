@@ -1,0 +1,86 @@
+// fl_mm_common.cu -- grid-size-independent multimode kernels (per-time
+// contractions for each built mode count, the per-slot control kernel) and
+// the table of evaluation rounds per grid size.
+#include "fl_mm.cuh"
+#include "fl_mm_launch.h"
+
+namespace fl {
+
+#define DECL(LOGN) cudaError_t mm_round_##LOGN(const MmRound&);
+DECL(6) DECL(7) DECL(8) DECL(9) DECL(10) DECL(11) DECL(12) DECL(13) DECL(14)
+#undef DECL
+
+MmRoundFn mm_round_launcher(int logn) {
+    static const MmRoundFn f[15] = {nullptr,     nullptr,     nullptr,     nullptr,    nullptr,
+                                    nullptr,     mm_round_6,  mm_round_7,  mm_round_8, mm_round_9,
+                                    mm_round_10, mm_round_11, mm_round_12, mm_round_13,
+                                    mm_round_14};
+    if (logn < 0 || logn > 14) return nullptr;
+    return f[logn];
+}
+
+bool mm_supported_modes(int M) { return M >= 2 && M <= 10; }
+
+__global__ void __launch_bounds__(kMmCtl)
+    mm_control_kernel(const MmDesc* __restrict__ descs, MmState* __restrict__ states,
+                      const int* __restrict__ active, int consume, int* __restrict__ ndone) {
+    __shared__ double red[32];
+    const int slot = active[blockIdx.x];
+    const MmDesc& d = descs[slot];
+    MmState st = states[slot];
+    MmCtl c{d, st, red, (size_t)d.N * d.M, d.N};
+    if (consume && mm_rhs_phase(st.phase) && st.phase != PH_EVAL_FWD && st.phase != PH_EVAL_ADJ)
+        c.consume();
+    __syncthreads();
+    c.advance();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        states[slot] = st;
+        if (ndone && st.phase == PH_DONE) atomicAdd(ndone, 1);
+    }
+}
+
+
+namespace {
+
+template <typename R, int M>
+cudaError_t contract_m(const MmRound& a, int which) {
+    const int n = which == 2 ? a.N * M : a.N;
+    const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);
+    mm_contract_kernel<R, M><<<grid, kMmTB, 0, a.stream>>>(static_cast<const MmDesc*>(a.desc),
+                                                          a.state, a.active, which);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t contract_r(const MmRound& a, int which) {
+    switch (a.M) {
+        case 2: return contract_m<R, 2>(a, which);
+        case 3: return contract_m<R, 3>(a, which);
+        case 4: return contract_m<R, 4>(a, which);
+        case 5: return contract_m<R, 5>(a, which);
+        case 6: return contract_m<R, 6>(a, which);
+        case 7: return contract_m<R, 7>(a, which);
+        case 8: return contract_m<R, 8>(a, which);
+        case 9: return contract_m<R, 9>(a, which);
+        case 10: return contract_m<R, 10>(a, which);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+cudaError_t mm_launch_contract(const MmRound& a, int which) {
+    // the forward contraction runs in the batch's forward precision; the
+    // adjoint passes in FP64
+    if (which == 0 && !a.fp64) return contract_r<float>(a, which);
+    return contract_r<double>(a, which);
+}
+
+cudaError_t mm_launch_control(const MmRound& a, int consume) {
+    mm_control_kernel<<<a.nactive, kMmCtl, 0, a.stream>>>(static_cast<const MmDesc*>(a.desc),
+                                                          a.state, a.active, consume, a.ndone);
+    return cudaGetLastError();
+}
+
+}  // namespace fl

@@ -19,7 +19,9 @@ enum SlotPhase : int {
     PH_ADJ_INIT = 4,
     PH_ADJ = 5,
     PH_FINAL = 6,
-    PH_DONE = 7
+    PH_DONE = 7,
+    PH_EVAL_FWD = 8,  // multimode: one forward RHS evaluation (unit parity)
+    PH_EVAL_ADJ = 9   // multimode: one adjoint RHS evaluation
 };
 
 // status codes (same values as the public FL_* codes)
@@ -85,6 +87,71 @@ struct SlotState {
     double az, adt, aqold;   // adjoint integrator
     double abstol_adj;
     double J;
+    long naccept, nreject, nf;
+    long a_naccept, a_nreject, a_nf;
+    long iters, a_iters;
+};
+
+// ---------------------------------------------------------------------------
+// Multimode (M > 1) slots.  One right-hand-side evaluation runs as a chain of
+// kernels over every active slot (mode transforms, pair convolutions, per-time
+// contractions), and a control kernel advances each slot's integrator between
+// evaluations.  Fields are mode-major: element (t, m) of an (Nt, M) field sits
+// at t + Nt*m, as in the reference's column-major arrays.
+struct MmDesc {
+    // tables shared by all slots of one problem; [0] float, [1] double
+    const double* Dturns;   // M*N: D/(2 pi), turns per metre
+    const void* Heff[2];    // cx: hR * (-1)^k
+    const void* ss[2];      // real: fftshift(ωs/ω0)
+    const void* tw[2];      // cx: exp(-2 pi i k / N)
+    const void* G[2];       // M*M*NP: G[(i*M + j)*NP + q] (pair q = (k <= l))
+    int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
+    double one_m_fR;
+    double L, reltol, abstol;
+    int mode, log_cost, nsave;
+    int phase_per_mode;     // gradient: 1 = one phase per (t, m); 0 = phase shared by the modes
+    int ck_cap, seg_cap, step_cap;
+    long max_iters;
+    // caller data
+    const double* zsave;
+    double* save_out;       // nsave * M*N complex doubles, lab frame
+    const double* u0;       // M*N complex doubles
+    const unsigned char* mask;  // N band mask
+    const double* lamL;     // M*N complex doubles
+    double* lam0_out;       // M*N complex doubles (nullable)
+    double* grad_out;       // N or M*N doubles (nullable)
+    double* uL_out;         // M*N complex doubles (nullable)
+    // integrator workspace
+    double* u[2];           // FP64 forward states
+    double* lam[2];         // FP64 adjoint states
+    void* kf[7];            // forward stages, cx<RF>
+    void* ka[7];            // adjoint stages, cx<double>
+    void* probe;            // initial-step probe derivative, cx<double>-sized
+    double* esv;            // error partial, M*N complex doubles
+    double* skv;            // error weights, M*N doubles
+    double* part;           // per-mode error sums (M doubles)
+    double* ck_u;           // ck_cap * M*N complex doubles
+    void* ck_k1;            // ck_cap * M*N cx<RF>
+    double* steplog;        // 2 * step_cap doubles
+    void* seg;              // seg_cap * 5 * M*N cx<RF>
+    // right-hand-side workspace (cx<double>-sized so both precisions fit)
+    void* ut;               // M*N: forward field in time
+    void* lt;               // M*N: adjoint field in time
+    void* sq;               // NP*N real: pair sequences S (forward) / S' (adjoint)
+    void* cq;               // NP*N real: adjoint Im X, then its Raman correlation
+    void* eta;              // M*N: nonlinear term in time
+};
+
+struct MmState {
+    int phase, status;
+    int cur, kperm, acur, akperm;
+    int nsteps, ck_stride, seg, save_idx, rec_pos, stage;
+    double cz, cdt, aprop;
+    double z, dt, qold;
+    double az, adt, aqold;
+    double abstol_adj, J;
+    double ez, ezload;      // position of the pending evaluation and of the forward field it reads
+    double dprobe;          // initial step: d1 of the launch
     long naccept, nreject, nf;
     long a_naccept, a_nreject, a_nf;
     long iters, a_iters;

@@ -25,7 +25,8 @@ EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_last_error", "fl_ctx_launch_count", "fl_ctx_synchronize", "fl_problem_create",
            "fl_problem_destroy", "fl_forward", "fl_adjoint", "fl_phase_gradient_batch",
            "fl_phase_gradient_batch_device", "fl_rhs_eval", "fl_ctx_timing",
-           "fl_forward_noalloc")
+           "fl_forward_noalloc", "fl_mode_phase_gradient_batch",
+           "fl_mode_phase_gradient_batch_device")
 
 
 class FlCtxOpts(C.Structure):
@@ -78,6 +79,8 @@ def load() -> C.CDLL:
         lib.fl_adjoint.argtypes = [vp, vp, vp, C.POINTER(FlStats)]
         lib.fl_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
+        lib.fl_mode_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
+        lib.fl_mode_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_rhs_eval.argtypes = [vp, ip, dp, vp, vp, vp]
         lib.fl_ctx_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.fl_forward_noalloc.argtypes = [ip, ip, vp, dp, vp, vp, dp, dp, dp, dp, vp, vp, ip,
@@ -198,6 +201,20 @@ class GPUProblem:
         st = (FlStats * B)()
         self.ctx.check(load().fl_phase_gradient_batch(self.h, _ptr(u0), B, _ptr(ph), _ptr(m),
                                                       int(log_cost), _ptr(J), _ptr(g), st))
+        return J, g, [s.as_dict() for s in st]
+
+    def mode_phase_gradient_batch(self, phases, mask=None, u0=None, log_cost=False):
+        """One phase per (mode, time bin): phases (B, M, Nt) -> J (B,), grad (B, M, Nt)."""
+        fp = self.fp
+        ph = np.ascontiguousarray(phases, dtype=np.float64).reshape(-1, fp.M, fp.nt)
+        B = ph.shape[0]
+        u0 = np.ascontiguousarray(fp.uw0 if u0 is None else u0, dtype=np.complex128)
+        m = np.ascontiguousarray(fp.mask if mask is None else mask, dtype=np.uint8)
+        J = np.empty(B)
+        g = np.empty((B, fp.M, fp.nt))
+        st = (FlStats * B)()
+        self.ctx.check(load().fl_mode_phase_gradient_batch(self.h, _ptr(u0), B, _ptr(ph), _ptr(m),
+                                                           int(log_cost), _ptr(J), _ptr(g), st))
         return J, g, [s.as_dict() for s in st]
 
     def phase_gradient_batch_device(self, d_u0: int, B: int, d_phases: int, d_mask: int,

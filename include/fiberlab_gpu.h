@@ -139,6 +139,15 @@ int fl_phase_gradient_batch(fl_problem *prob, const double *u0, int nbatch,
                             const double *phases, const unsigned char *mask, int log_cost,
                             double *J, double *grad, fl_stats *stats);
 
+/* Same as fl_phase_gradient_batch with one phase per (time bin, mode): the
+ * matrix-phase control of _phase_matrix (physics_models.jl:685-704) whose
+ * gradient keeps the mode axis.
+ *   phases  (Nt, M, nbatch); grad (Nt, M, nbatch) ∂J/∂φ[t, m].
+ * For M = 1 this is fl_phase_gradient_batch. */
+int fl_mode_phase_gradient_batch(fl_problem *prob, const double *u0, int nbatch,
+                                 const double *phases, const unsigned char *mask, int log_cost,
+                                 double *J, double *grad, fl_stats *stats);
+
 /* One evaluation of the forward right-hand side disp_mmf!
  * (simulate_disp_mmf.jl:25-60) or, with adjoint = 1, of adjoint_disp_mmf!
  * (sensitivity_disp_mmf.jl:32-79) with the forward field u_fwd given
@@ -152,6 +161,12 @@ int fl_phase_gradient_batch_device(fl_problem *prob, const double *d_u0, int nba
                                    const double *d_phases, const unsigned char *d_mask,
                                    int log_cost, double *d_J, double *d_grad,
                                    fl_stats *stats);
+
+/* Device-pointer form of fl_mode_phase_gradient_batch. */
+int fl_mode_phase_gradient_batch_device(fl_problem *prob, const double *d_u0, int nbatch,
+                                        const double *d_phases, const unsigned char *d_mask,
+                                        int log_cost, double *d_J, double *d_grad,
+                                        fl_stats *stats);
 
 /* Forward solve that allocates no device memory.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc -- host runtimes
