@@ -130,6 +130,7 @@ struct fl_problem {
     int nt = 0, m = 0, precision = 0;
     double one_m_fR = 0, L = 0, reltol = 0, abstol = 0, gamma0 = 0;
     bool gamma_sym = true;
+    bool use_mm = false;  // multimode runtime: M > 1, or M = 1 beyond one CTA's transform (2^15)
     double* d_Dturns = nullptr;
     void* d_Heff[2] = {nullptr, nullptr};  // [0] float, [1] double
     void* d_ss[2] = {nullptr, nullptr};
@@ -435,12 +436,12 @@ struct MmWork {
 
 namespace {
 
-size_t mm_slot_bytes(size_t nm, size_t npn, size_t rf, int K, int segcap, int stepcap, int M) {
+size_t mm_slot_bytes(size_t nm, size_t npn, size_t rf, int K, int segcap, int stepcap, int nparts) {
     const size_t C = 2 * rf * nm, D2 = 16 * nm;
     size_t b = 0;
     b += 4 * D2;                         // u[2], lam[2]
     b += 7 * C + 7 * D2;                 // kf, ka
-    b += 2 * D2 + 8 * nm + 8 * (size_t)M;  // probe, esv, skv, part
+    b += 2 * D2 + 8 * nm + 8 * (size_t)nparts;  // probe, esv, skv, part
     b += (size_t)K * (D2 + C);           // checkpoints
     b += 16 * (size_t)stepcap;           // step log
     b += (size_t)segcap * 5 * C;         // recompute segment
@@ -463,7 +464,8 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     w->nsave = nsave;
     w->per_mode = per_mode;
     const size_t nm = (size_t)pr->nt * pr->m, npn = (size_t)w->np * pr->nt;
-    const size_t per = mm_slot_bytes(nm, npn, rf, w->K, w->segcap, w->stepcap, pr->m);
+    const int nparts = pr->m * mm_cluster_ctas(ilog2i(pr->nt));
+    const size_t per = mm_slot_bytes(nm, npn, rf, w->K, w->segcap, w->stepcap, nparts);
     const size_t io = 16 * nm * (4 + nsave) + 8 * nm + 256 * 8;
     w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + pr->nt + 4096;
     if (ctx->opts.hbm_budget_bytes && w->pool_bytes > ctx->opts.hbm_budget_bytes)
@@ -496,6 +498,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
             d.G[q] = pr->d_G[q];
         }
         d.M = pr->m;
+        d.nparts = nparts;
         d.NP = w->np;
         d.N = pr->nt;
         d.fp64 = pr->precision == FL_PRECISION_FP64;
@@ -526,7 +529,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         d.probe = carve(p, D2);
         d.esv = (double*)carve(p, D2);
         d.skv = (double*)carve(p, 8 * nm);
-        d.part = (double*)carve(p, 8 * (size_t)pr->m);
+        d.part = (double*)carve(p, 8 * (size_t)nparts);
         d.ck_u = (double*)carve(p, D2 * w->K);
         d.ck_k1 = carve(p, C * w->K);
         d.steplog = (double*)carve(p, 16 * (size_t)w->stepcap);
@@ -941,12 +944,13 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
     pr->abstol = abstol;
     pr->gamma0 = gamma[0];
     pr->gamma_sym = gamma_symmetric(gamma, m);
-    if (m > 1 && (!mm_supported_modes(m) || !mm_round_launcher(ilog2i(nt))))
-        return set_err(ctx, FL_EUNSUPPORTED, "multimode problems are built for M = 2..10 and "
-                       "Nt = 2^6..2^14 (got M = %d, Nt = %d)", m, nt);
+    pr->use_mm = m > 1 || ilog2i(nt) > 14;
+    if (pr->use_mm && ((m > 1 && !mm_supported_modes(m)) || !mm_round_launcher(ilog2i(nt))))
+        return set_err(ctx, FL_EUNSUPPORTED, "built shapes: M = 1 with Nt = 2^6..2^15, "
+                       "M = 2..10 with Nt = 2^6..2^15 (got M = %d, Nt = %d)", m, nt);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
     int rc = upload_tables(pr.get(), D, hR, selfsteep);
-    if (!rc && m > 1) rc = mm_upload_G(pr.get(), gamma);
+    if (!rc && pr->use_mm) rc = mm_upload_G(pr.get(), gamma);
     if (rc) {
         fl_problem_destroy(pr.release());
         return rc;
@@ -997,7 +1001,7 @@ int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave
     }
     if (!(nrm > 0)) return set_err(ctx, FL_EINVAL, "input spectrum must be nonzero");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
-    if (pr->m > 1) return mm_forward(pr, u0, saveat, nsave, out_spectra, stats);
+    if (pr->use_mm) return mm_forward(pr, u0, saveat, nsave, out_spectra, stats);
     delete pr->last;
     pr->last = nullptr;
     Work* w = nullptr;
@@ -1028,14 +1032,14 @@ int fl_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats*
     if (!pr->gamma_sym)
         return set_err(ctx, FL_NONSYMMETRIC,
                        "fiber adjoint requires a fully permutation-symmetric gamma tensor");
-    if (!(pr->m > 1 ? (void*)pr->mlast : (void*)pr->last))
+    if (!(pr->use_mm ? (void*)pr->mlast : (void*)pr->last))
         return set_err(ctx, FL_EINVAL, "fl_adjoint needs a preceding fl_forward");
     const int nt = pr->nt;
     for (int i = 0; i < 2 * nt * pr->m; i++)
         if (!std::isfinite(lambdaL[i]))
             return set_err(ctx, FL_EINVAL, "adjoint terminal condition must be finite");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
-    if (pr->m > 1) return mm_adjoint(pr, lambdaL, lambda0, stats);
+    if (pr->use_mm) return mm_adjoint(pr, lambdaL, lambda0, stats);
     Work* w = pr->last;
     std::vector<SlotState> st;
     rc = read_states(ctx, w, st);
@@ -1069,7 +1073,7 @@ int fl_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const
         return set_err(ctx, FL_NONSYMMETRIC,
                        "fiber adjoint requires a fully permutation-symmetric gamma tensor");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
-    if (pr->m > 1) return mm_rhs_eval(pr, adjoint, z, u_in, u_fwd, du_out);
+    if (pr->use_mm) return mm_rhs_eval(pr, adjoint, z, u_in, u_fwd, du_out);
     const int fp64 = pr->precision == FL_PRECISION_FP64;
     RhsFn fn = rhs_launcher(fp64, ilog2i(pr->nt));
     if (!fn) return set_err(ctx, FL_EUNSUPPORTED, "Nt = %d is not built", pr->nt);
@@ -1139,9 +1143,9 @@ static int phase_gradient_device(fl_problem* pr, const double* d_u0, int nbatch,
         return set_err(ctx, FL_NONSYMMETRIC,
                        "fiber adjoint requires a fully permutation-symmetric gamma tensor");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
-    if (pr->m > 1)
-        return mm_phase_gradient_device(pr, d_u0, nbatch, d_phases, per_mode, d_mask, log_cost,
-                                        d_J, d_grad, stats);
+    if (pr->use_mm)
+        return mm_phase_gradient_device(pr, d_u0, nbatch, d_phases, per_mode && pr->m > 1, d_mask,
+                                        log_cost, d_J, d_grad, stats);
     // single mode: a per-mode phase is the shared phase
     // keep one workspace per problem sized for the largest batch seen
     if (!pr->last || pr->last->B < nbatch || pr->last->nsave != 0) {

@@ -37,6 +37,7 @@
 // RF (FP32 by default) with FP64 phase arguments, state, error norm and
 // reductions; the adjoint runs in FP64.
 #pragma once
+#include "fl_cfft.cuh"
 #include "fl_sm.cuh"
 #include "fl_types.h"
 
@@ -89,43 +90,65 @@ __device__ __forceinline__ void stcr(void* p, size_t i, cx<double> v, bool fp64)
     else static_cast<cx<float>*>(p)[i] = down<float>(v);
 }
 
-// shared memory of the transform kernels: [exchange buffer][twiddles][32 doubles]
-template <typename R, int LOGN>
-constexpr size_t mm_smem_bytes() {
-    return SmemPlan<R, LOGN>::BYTES + sizeof(cx<R>) * Twiddles<R, LOGN>::SIZE + 32 * sizeof(double);
-}
+// One transform group: a CTA (C = 1) or a cluster of C CTAs (see
+// fl_cfft.cuh).  g is the thread's index in the group, TT the group's thread
+// count; a thread owns the positions g + TT*s.
+template <typename R, int LOGN, int LOGE, int C>
+struct MmGroup {
+    using CS = ClusterShape<LOGN, LOGE, C>;
+    static constexpr int N = CS::N, E = CS::E, TT = CS::TT, T = CS::T;
+    // per-CTA exchange buffer bytes
+    static constexpr size_t XBYTES =
+        C == 1 ? SmemPlan<R, LOGN>::BYTES : cluster_xbytes<R, LOGN, C>();
+    static constexpr size_t SMEM =
+        XBYTES + sizeof(cx<R>) * Twiddles<R, LOGN>::SIZE + 32 * sizeof(double);
+    int rank, g;
+    unsigned char* sm;
+    double* red;
+    Twiddles<R, LOGN> tw;
 
-template <typename R, int LOGN>
-__device__ __forceinline__ Twiddles<R, LOGN> mm_load_twiddles(const MmDesc& d, unsigned char* smraw,
-                                                              double*& red) {
-    cx<R>* tws = reinterpret_cast<cx<R>*>(smraw + SmemPlan<R, LOGN>::BYTES);
-    red = reinterpret_cast<double*>(tws + Twiddles<R, LOGN>::SIZE);
-    Twiddles<R, LOGN>::fill(tws, static_cast<const cx<R>*>(d.tw[sizeof(R) == 8]));
-    __syncthreads();
-    return Twiddles<R, LOGN>::at(tws);
-}
+    __device__ __forceinline__ void sync() const {
+        if constexpr (C == 1) __syncthreads();
+        else cluster_sync_all();
+    }
+    // every CTA of the group calls it (uniform early exits only before it)
+    __device__ __forceinline__ void init(const MmDesc& d, unsigned char* smraw) {
+        rank = C == 1 ? 0 : (int)(blockIdx.x % C);
+        g = rank * T + threadIdx.x;
+        sm = smraw;
+        cx<R>* tws = reinterpret_cast<cx<R>*>(smraw + XBYTES);
+        red = reinterpret_cast<double*>(tws + Twiddles<R, LOGN>::SIZE);
+        Twiddles<R, LOGN>::fill(tws, static_cast<const cx<R>*>(d.tw[sizeof(R) == 8]));
+        sync();
+        tw = Twiddles<R, LOGN>::at(tws);
+    }
+    __device__ __forceinline__ void fft(cx<R> (&v)[E]) const {
+        if constexpr (C == 1) block_fft<R, LOGN, LOGE>(v, sm, tw);
+        else cluster_fft<R, LOGN, LOGE, C>(v, reinterpret_cast<cx<R>*>(sm), tw, g);
+    }
+};
 
 // ---------------------------------------------------------------------------
 // prologue: stage input of mode m and its transform(s) to time
 // ---------------------------------------------------------------------------
-template <typename R, int LOGN, int LOGE>
-__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+template <typename R, int LOGN, int LOGE, int CL>
+__global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     mm_prologue_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
                        const int* __restrict__ active) {
-    using S = FftShape<LOGN, LOGE>;
-    constexpr int N = S::N, E = S::E, T = S::T;
+    using G = MmGroup<R, LOGN, LOGE, CL>;
+    constexpr int N = G::N, E = G::E, T = G::T, TT = G::TT;
     constexpr int P = sizeof(R) == 8;
     using C = cx<R>;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
-    const int m = blockIdx.x;
+    const int m = blockIdx.x / CL;
     if (m >= d.M) return;
     const MmState st = states[slot];
     if (!mm_takes<R>(d, st)) return;
-    double* red;
-    const Twiddles<R, LOGN> tw = mm_load_twiddles<R, LOGN>(d, smraw, red);
-    const int tid = threadIdx.x;
+    G grp;
+    grp.init(d, smraw);
+    const int tid = grp.g;  // index in the transform group
     const size_t NM = (size_t)N * d.M, off = (size_t)m * N;
     const int ph = st.phase;
     const bool adj = mm_adjoint_phase(ph);
@@ -134,7 +157,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     // ---- stage input (FP64 accumulation, as the single-mode stepper)
     if (ph == PH_EVAL_FWD || ph == PH_EVAL_ADJ) {
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.u0, off + tid + T * s));
+        for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.u0, off + tid + TT * s));
     } else if (ph == PH_FWD_INIT || ph == PH_ADJ_INIT) {
         const bool fw = ph == PH_FWD_INIT;
         const double* x0 = fw ? d.u0 : d.lam[0];
@@ -142,7 +165,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         const double sg = fw ? st.cdt : -st.cdt;
 #pragma unroll
         for (int s = 0; s < E; s++) {
-            const size_t b = off + tid + T * s;
+            const size_t b = off + tid + TT * s;
             const cx<double> x = ld2(x0, b);
             if (st.stage == 0) {
                 v[s] = down<R>(x);
@@ -161,7 +184,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         if (st.stage < 6) {
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const size_t b = off + tid + T * s;
+                const size_t b = off + tid + TT * s;
                 double ar = 0.0, ai = 0.0;
                 for (int j = 0; j < st.stage; j++) {
                     const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
@@ -178,7 +201,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double at = fw ? d.abstol : st.abstol_adj, rt = d.reltol;
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const size_t b = off + tid + T * s;
+                const size_t b = off + tid + TT * s;
                 double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
                 for (int j = 0; j < 6; j++) {
                     const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
@@ -208,19 +231,19 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     C* out = static_cast<C*>(adj ? d.lt : d.ut);
 #pragma unroll
     for (int s = 0; s < E; s++) {
-        const int t = tid + T * s;
+        const int t = tid + TT * s;
         v[s] = cmul(v[s], phasor<R>(Dt[t], st.ez));
         if (adj) v[s] = scale(v[s], ss[t]);
     }
-    block_fft<R, LOGN, LOGE>(v, smraw, tw);
+    grp.fft(v);
 #pragma unroll
-    for (int s = 0; s < E; s++) out[off + tid + T * s] = v[s];
+    for (int s = 0; s < E; s++) out[off + tid + TT * s] = v[s];
     if (!adj) return;
 
     // ---- adjoint: the forward field at ezload, F(e^{iDz} ũ(z))
     if (ph == PH_EVAL_ADJ) {
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.lamL, off + tid + T * s));
+        for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.lamL, off + tid + TT * s));
     } else {
         const int seg_lo = st.seg * st.ck_stride;
         const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
@@ -233,7 +256,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         const size_t base = (size_t)(n - seg_lo) * 5 * NM;
 #pragma unroll
         for (int s = 0; s < E; s++) {
-            const size_t b = off + tid + T * s;
+            const size_t b = off + tid + TT * s;
             cx<double> c[5];
 #pragma unroll
             for (int q = 0; q < 5; q++) c[q] = ldcr(d.seg, base + q * NM + b, d.fp64);
@@ -242,13 +265,13 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             v[s] = mk((R)xr, (R)xi);
         }
     }
-    __syncthreads();  // the exchange buffer is reused
+    grp.sync();  // the exchange buffer is reused
 #pragma unroll
-    for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(Dt[tid + T * s], st.ez));
-    block_fft<R, LOGN, LOGE>(v, smraw, tw);
+    for (int s = 0; s < E; s++) v[s] = cmul(v[s], phasor<R>(Dt[tid + TT * s], st.ez));
+    grp.fft(v);
     C* uo = static_cast<C*>(d.ut);
 #pragma unroll
-    for (int s = 0; s < E; s++) uo[off + tid + T * s] = v[s];
+    for (int s = 0; s < E; s++) uo[off + tid + TT * s] = v[s];
 }
 
 // ---------------------------------------------------------------------------
@@ -260,12 +283,12 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 // [ceil(NP/2), 2 ceil(NP/2)) the Im X_q: packing P (~|u_t|²) with the much
 // smaller Im X would leave Im X with the rounding of P.
 // ---------------------------------------------------------------------------
-template <typename R, int LOGN, int LOGE>
-__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+template <typename R, int LOGN, int LOGE, int CL>
+__global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     mm_pairs_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
                     const int* __restrict__ active) {
-    using S = FftShape<LOGN, LOGE>;
-    constexpr int N = S::N, E = S::E, T = S::T;
+    using G = MmGroup<R, LOGN, LOGE, CL>;
+    constexpr int N = G::N, E = G::E, T = G::T, TT = G::TT;
     constexpr int P = sizeof(R) == 8;
     using C = cx<R>;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -275,15 +298,16 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     if (!mm_takes<R>(d, st)) return;
     const bool adj = mm_adjoint_phase(st.phase);
     const int M = d.M, NP = d.NP, ntp = (NP + 1) / 2;
-    const bool ytask = (int)blockIdx.x >= ntp;  // correlation of Im X (adjoint only)
+    const int unit = blockIdx.x / CL;
+    const bool ytask = unit >= ntp;  // correlation of Im X (adjoint only)
     if (ytask && !adj) return;
-    const int q0 = 2 * (ytask ? blockIdx.x - ntp : blockIdx.x);
+    const int q0 = 2 * (ytask ? unit - ntp : unit);
     if (q0 >= NP) return;
     const int q1 = q0 + 1;
     const bool two = q1 < NP;
-    double* red;
-    const Twiddles<R, LOGN> tw = mm_load_twiddles<R, LOGN>(d, smraw, red);
-    const int tid = threadIdx.x;
+    G grp;
+    grp.init(d, smraw);
+    const int tid = grp.g;  // index in the transform group
     const C* ut = static_cast<const C*>(d.ut);
     const C* H = static_cast<const C*>(d.Heff[P]);
     R* sq = static_cast<R*>(d.sq);
@@ -296,7 +320,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     R p0[E], p1[E];
 #pragma unroll
     for (int s = 0; s < E; s++) {
-        const int t = tid + T * s;
+        const int t = tid + TT * s;
         if (ytask) {
             p0[s] = cq[(size_t)q0 * N + t];
             p1[s] = two ? cq[(size_t)q1 * N + t] : R(0);
@@ -312,20 +336,20 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         }
         v[s] = mk(p0[s], p1[s]);
     }
-    block_fft<R, LOGN, LOGE>(v, smraw, tw);
+    grp.fft(v);
 #pragma unroll
     for (int s = 0; s < E; s++) {
-        const C h = H[tid + T * s];
+        const C h = H[tid + TT * s];
         v[s] = ytask ? cmulc(v[s], h) : cmul(v[s], h);  // conj(Heff): correlation
     }
     conj_all(v);
-    block_fft<R, LOGN, LOGE>(v, smraw, tw);
+    grp.fft(v);
     conj_all(v);
     // forward S = (1-fR) P + h∗P; adjoint S' = 2(1-fR) P + h∗P and C = h̃⋆Im X
     const R kf = adj ? R(2) * ofr : ofr;
 #pragma unroll
     for (int s = 0; s < E; s++) {
-        const int t = tid + T * s;
+        const int t = tid + TT * s;
         if (ytask) {
             cq[(size_t)q0 * N + t] = v[s].re * invn;
             if (two) cq[(size_t)q1 * N + t] = v[s].im * invn;
@@ -340,45 +364,45 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 // epilogue: nonlinear term of mode m back to the interaction frame, stored
 // as the stage derivative; the stage-7 error partial of the mode
 // ---------------------------------------------------------------------------
-template <typename R, int LOGN, int LOGE>
-__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+template <typename R, int LOGN, int LOGE, int CL>
+__global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     mm_epilogue_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
                        const int* __restrict__ active) {
-    using S = FftShape<LOGN, LOGE>;
-    constexpr int N = S::N, E = S::E, T = S::T;
+    using G = MmGroup<R, LOGN, LOGE, CL>;
+    constexpr int N = G::N, E = G::E, T = G::T, TT = G::TT;
     constexpr int P = sizeof(R) == 8;
     using C = cx<R>;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
-    const int m = blockIdx.x;
+    const int m = blockIdx.x / CL;
     if (m >= d.M) return;
     const MmState st = states[slot];
     if (!mm_takes<R>(d, st)) return;
-    double* red;
-    const Twiddles<R, LOGN> tw = mm_load_twiddles<R, LOGN>(d, smraw, red);
-    const int tid = threadIdx.x;
+    G grp;
+    grp.init(d, smraw);
+    const int tid = grp.g;  // index in the transform group
     const size_t off = (size_t)m * N;
     const int ph = st.phase;
     const bool adj = mm_adjoint_phase(ph);
     const C* eta = static_cast<const C*>(d.eta);
     C v[E];
 #pragma unroll
-    for (int s = 0; s < E; s++) v[s] = conjc(eta[off + tid + T * s]);
-    block_fft<R, LOGN, LOGE>(v, smraw, tw);
+    for (int s = 0; s < E; s++) v[s] = conjc(eta[off + tid + TT * s]);
+    grp.fft(v);
     const double* Dt = d.Dturns + off;
     const R* ss = static_cast<const R*>(d.ss[P]);
     const R invn = R(1) / R(N);
 #pragma unroll
     for (int s = 0; s < E; s++) {
-        const int t = tid + T * s;
+        const int t = tid + TT * s;
         const C y = cmulc(conjc(v[s]), phasor<R>(Dt[t], st.ez));  // e^{-iDz} x
         const R sc = adj ? invn : ss[t] * invn;
         v[s] = mk(-y.im * sc, y.re * sc);  // i y (τ) / N
     }
     if (ph == PH_EVAL_FWD || ph == PH_EVAL_ADJ) {
 #pragma unroll
-        for (int s = 0; s < E; s++) st2(d.lam0_out, off + tid + T * s, up(v[s]));
+        for (int s = 0; s < E; s++) st2(d.lam0_out, off + tid + TT * s, up(v[s]));
         return;
     }
     C* dst;
@@ -387,21 +411,21 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     else if (adj) dst = static_cast<C*>(mm_kp(d.ka, st.akperm, st.stage));
     else dst = static_cast<C*>(mm_kp(d.kf, st.kperm, st.stage));
 #pragma unroll
-    for (int s = 0; s < E; s++) dst[off + tid + T * s] = v[s];
+    for (int s = 0; s < E; s++) dst[off + tid + TT * s] = v[s];
     if (st.stage == 6 && (ph == PH_FWD || ph == PH_ADJ)) {
         const double dt = st.cdt, bt7 = kT5bt[6];
         double acc = 0.0;
 #pragma unroll
         for (int s = 0; s < E; s++) {
-            const size_t b = off + tid + T * s;
+            const size_t b = off + tid + TT * s;
             const cx<double> e6 = ld2(d.esv, b);
             const double er = e6.re + dt * bt7 * (double)v[s].re;
             const double ei = e6.im + dt * bt7 * (double)v[s].im;
             const double w = d.skv[b];
             acc += (er * er + ei * ei) / (w * w);
         }
-        const double tot = block_sum<T>(acc, red);
-        if (tid == 0) d.part[m] = tot;
+        const double tot = block_sum<T>(acc, grp.red);
+        if (threadIdx.x == 0) d.part[m * CL + grp.rank] = tot;
     }
 }
 
@@ -723,7 +747,7 @@ struct MmCtl {
                 return;
             }
             double acc = 0.0;
-            for (int m = 0; m < d.M; m++) acc += d.part[m];
+            for (int m = 0; m < d.nparts; m++) acc += d.part[m];
             const double EEst = sqrt(acc / (double)NM);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;
@@ -819,7 +843,7 @@ struct MmCtl {
             const double z = st.cz, dt = st.cdt;
             const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
             double acc = 0.0;
-            for (int m = 0; m < d.M; m++) acc += d.part[m];
+            for (int m = 0; m < d.nparts; m++) acc += d.part[m];
             const double EEst = sqrt(acc / (double)NM);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;

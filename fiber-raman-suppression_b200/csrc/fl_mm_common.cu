@@ -7,17 +7,19 @@
 namespace fl {
 
 #define DECL(LOGN) cudaError_t mm_round_##LOGN(const MmRound&);
-DECL(6) DECL(7) DECL(8) DECL(9) DECL(10) DECL(11) DECL(12) DECL(13) DECL(14)
+DECL(6) DECL(7) DECL(8) DECL(9) DECL(10) DECL(11) DECL(12) DECL(13) DECL(14) DECL(15)
 #undef DECL
 
 MmRoundFn mm_round_launcher(int logn) {
-    static const MmRoundFn f[15] = {nullptr,     nullptr,     nullptr,     nullptr,    nullptr,
+    static const MmRoundFn f[16] = {nullptr,     nullptr,     nullptr,     nullptr,    nullptr,
                                     nullptr,     mm_round_6,  mm_round_7,  mm_round_8, mm_round_9,
                                     mm_round_10, mm_round_11, mm_round_12, mm_round_13,
-                                    mm_round_14};
-    if (logn < 0 || logn > 14) return nullptr;
+                                    mm_round_14, mm_round_15};
+    if (logn < 0 || logn > 15) return nullptr;
     return f[logn];
 }
+
+int mm_cluster_ctas(int logn) { return logn == 15 ? 4 : 1; }
 
 bool mm_supported_modes(int M) { return M >= 2 && M <= 10; }
 
@@ -55,6 +57,7 @@ cudaError_t contract_m(const MmRound& a, int which) {
 template <typename R>
 cudaError_t contract_r(const MmRound& a, int which) {
     switch (a.M) {
+        case 1: return contract_m<R, 1>(a, which);
         case 2: return contract_m<R, 2>(a, which);
         case 3: return contract_m<R, 3>(a, which);
         case 4: return contract_m<R, 4>(a, which);

@@ -5,34 +5,54 @@
 
 namespace fl {
 
-template <typename R, int LOGN, int LOGE>
+// which: 0 prologue, 1 pairs, 2 epilogue; CL CTAs (one cluster) per transform
+template <typename R, int LOGN, int LOGE, int CL>
 cudaError_t mm_launch_fft_kernels(const MmRound& a, int which) {
-    using S = FftShape<LOGN, LOGE>;
-    const size_t smem = mm_smem_bytes<R, LOGN>();
+    using G = MmGroup<R, LOGN, LOGE, CL>;
+    const size_t smem = G::SMEM;
     void (*k)(const MmDesc*, const MmState*, const int*) =
-        which == 0 ? mm_prologue_kernel<R, LOGN, LOGE>
-                   : which == 1 ? mm_pairs_kernel<R, LOGN, LOGE> : mm_epilogue_kernel<R, LOGN, LOGE>;
+        which == 0   ? mm_prologue_kernel<R, LOGN, LOGE, CL>
+        : which == 1 ? mm_pairs_kernel<R, LOGN, LOGE, CL>
+                     : mm_epilogue_kernel<R, LOGN, LOGE, CL>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const dim3 grid(which == 1 ? 2 * ((a.NP + 1) / 2) : a.M, a.nactive);
-    k<<<grid, S::T, smem, a.stream>>>(static_cast<const MmDesc*>(a.desc), a.state, a.active);
-    return cudaGetLastError();
+    const int units = which == 1 ? 2 * ((a.NP + 1) / 2) : a.M;
+    const dim3 grid(units * CL, a.nactive);
+    if constexpr (CL == 1) {
+        k<<<grid, G::T, smem, a.stream>>>(static_cast<const MmDesc*>(a.desc), a.state, a.active);
+        return cudaGetLastError();
+    } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = dim3(G::T);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = a.stream;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k, static_cast<const MmDesc*>(a.desc),
+                                  static_cast<const MmState*>(a.state), a.active);
+    }
 }
 
-template <int LOGN, int LOGE>
+template <int LOGN, int LOGE, int CL>
 cudaError_t mm_round(const MmRound& a) {
     cudaError_t e;
 #define FL_TRY(x)                        \
     if ((e = (x)) != cudaSuccess) return e;
-    if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE>(a, 0)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE>(a, 0)));
+    if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 0)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 0)));
     FL_TRY(mm_launch_contract(a, 1));
-    if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE>(a, 1)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE>(a, 1)));
+    if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 1)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 1)));
     FL_TRY(mm_launch_contract(a, 0));
     FL_TRY(mm_launch_contract(a, 2));
-    if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE>(a, 2)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE>(a, 2)));
+    if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 2)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 2)));
     if (a.control) FL_TRY(mm_launch_control(a, 1));
 #undef FL_TRY
     return cudaSuccess;
@@ -40,7 +60,7 @@ cudaError_t mm_round(const MmRound& a) {
 
 }  // namespace fl
 
-#define FL_MM_INSTANCE(LOGN, LOGE)                                                   \
-    namespace fl {                                                                   \
-    cudaError_t mm_round_##LOGN(const MmRound& a) { return mm_round<LOGN, LOGE>(a); } \
+#define FL_MM_INSTANCE(LOGN, LOGE, CL)                                                     \
+    namespace fl {                                                                         \
+    cudaError_t mm_round_##LOGN(const MmRound& a) { return mm_round<LOGN, LOGE, CL>(a); } \
     }

@@ -28,5 +28,7 @@ MmRoundFn mm_round_launcher(int logn);
 cudaError_t mm_launch_contract(const MmRound& a, int which);  // 0 fwd, 1 Im X, 2 adjoint
 cudaError_t mm_launch_control(const MmRound& a, int consume);
 bool mm_supported_modes(int M);
+// CTAs (one cluster) per transform at Nt = 2^logn
+int mm_cluster_ctas(int logn);
 
 }  // namespace fl

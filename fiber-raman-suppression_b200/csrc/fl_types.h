@@ -106,6 +106,7 @@ struct MmDesc {
     const void* tw[2];      // cx: exp(-2 pi i k / N)
     const void* G[2];       // M*M*NP: G[(i*M + j)*NP + q] (pair q = (k <= l))
     int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
+    int nparts;             // error partial sums per evaluation (M x CTAs per transform)
     double one_m_fR;
     double L, reltol, abstol;
     int mode, log_cost, nsave;
@@ -129,7 +130,7 @@ struct MmDesc {
     void* probe;            // initial-step probe derivative, cx<double>-sized
     double* esv;            // error partial, M*N complex doubles
     double* skv;            // error weights, M*N doubles
-    double* part;           // per-mode error sums (M doubles)
+    double* part;           // error partial sums (nparts doubles)
     double* ck_u;           // ck_cap * M*N complex doubles
     void* ck_k1;            // ck_cap * M*N cx<RF>
     double* steplog;        // 2 * step_cap doubles

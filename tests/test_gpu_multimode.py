@@ -169,27 +169,50 @@ def test_mm_gradient_central_differences(gpu_ctx):
 
 def test_mm_config4_shape_properties(gpu_ctx):
     # M = 10 HG(m+n<=3) on a 96x96 grid, Nt = 2^14 over 10 ps, L = 2 m, 5 nJ,
-    # 64 per-mode phase candidates φ ~ N(0, 1): run as one batch; check 4
-    # candidates alone against the batch (bit-identical) and their gradients
-    # against central differences of FP64 GPU forwards along a random direction
+    # 64 per-mode phase candidates φ ~ N(0, 1) run as one batch.  Checked on
+    # 4 candidates: alone against the batch (bit-identical), and the FP32
+    # gradient against the FP64-mode gradient of the same candidate (the
+    # oracle-validated algorithm in FP64; the CPU oracle itself would take
+    # tens of minutes per candidate at this size).  The band is the red side
+    # beyond 2 THz (J ~ 1e-2).
     fp = P.multimode_problem(3, 96, 16384, 10.0, 2.0, 5e-9, 200e-15, seed=0,
-                             raman_threshold_thz=-5.0)
+                             raman_threshold_thz=-2.0)
     assert fp.M == 10
     rng = np.random.default_rng(4)
     phases = rng.standard_normal((64, 10, fp.nt))
-    gp = GPUProblem(gpu_ctx, fp)
-    J, g, st = gp.mode_phase_gradient_batch(phases)
+    J, g, st = GPUProblem(gpu_ctx, fp).mode_phase_gradient_batch(phases)
     assert all(s["status"] == 0 for s in st)
-    gp64 = GPUProblem(gpu_ctx, fp, "fp64")
-
-    def cost(ph):
-        out, _ = gp64.forward(fp.uw0 * np.exp(1j * ph))
-        return P.band_cost_and_seed(out[-1], fp.mask)[0]
-    for b in (0, 21, 42, 63):
+    pick = [0, 21, 42, 63]
+    J64, g64, _ = GPUProblem(gpu_ctx, fp, "fp64").mode_phase_gradient_batch(phases[pick])
+    for n, b in enumerate(pick):
         Ja, ga, _ = GPUProblem(gpu_ctx, fp).mode_phase_gradient_batch(phases[b:b + 1])
         assert Ja[0] == J[b] and np.array_equal(ga[0], g[b])
-        d = rng.standard_normal((10, fp.nt))
+        assert abs(10 * np.log10(J[b]) - 10 * np.log10(J64[n])) < DB_TOL
+        assert rel(g[b], g64[n]) < GRAD_TOL
+
+
+def test_mm_config4_gradient_central_differences(gpu_ctx):
+    # The adjoint gradient against central differences (h = 1e-4) on the
+    # config-4 shape, both in FP64 mode at tight tolerances (reltol 1e-10,
+    # abstol 1e-9): at the default tolerances the two sides differ by their
+    # integration error (1e-4 .. 1e-3 on this 10-mode, 2 m problem), which
+    # is not what the check is after.  Directions mix a random unit vector
+    # with the gradient direction so that J(φ ± h d) differ well above the
+    # solves' noise.
+    fp = P.multimode_problem(3, 96, 16384, 10.0, 2.0, 5e-9, 200e-15, seed=0,
+                             raman_threshold_thz=-2.0, reltol=1e-10, abstol=1e-9)
+    rng = np.random.default_rng(44)
+    ph = rng.standard_normal((10, fp.nt))
+    gp64 = GPUProblem(gpu_ctx, fp, "fp64")
+    J, g, _ = gp64.mode_phase_gradient_batch(ph[None])
+
+    def cost(p):
+        out, _ = gp64.forward(fp.uw0 * np.exp(1j * p))
+        return P.band_cost_and_seed(out[-1], fp.mask)[0]
+    for _ in range(2):
+        r = rng.standard_normal((10, fp.nt))
+        d = r / np.linalg.norm(r) + g[0] / np.linalg.norm(g[0])
         d /= np.linalg.norm(d)
         h = 1e-4
-        fd = (cost(phases[b] + h * d) - cost(phases[b] - h * d)) / (2 * h)
-        assert abs(fd - np.sum(g[b] * d)) <= GRAD_TOL * abs(fd) + 1e-12
+        fd = (cost(ph + h * d) - cost(ph - h * d)) / (2 * h)
+        assert abs(fd - np.sum(g[0] * d)) <= GRAD_TOL * abs(fd)

@@ -26,11 +26,12 @@ def cfg0(nt=8192, T=10.0, **kw):
                                  rep_rate_hz=80e6, validate_grid=False, **kw)
 
 
-@pytest.mark.parametrize("nt", [64, 256, 1024, 8192, 16384])
+@pytest.mark.parametrize("nt", [64, 256, 1024, 8192, 16384, 32768])
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_rhs_matches_oracle(gpu_ctx, nt, precision):
-    if precision == "fp64" and nt > 8192:
-        pytest.skip("FP64 mode is built up to 2^13")
+    # 2^15 runs on the cluster transform of the multimode runtime (4 CTAs)
+    if precision == "fp64" and nt == 16384:
+        pytest.skip("FP64 mode is built up to 2^13 on one CTA, and at 2^15 on a cluster")
     fp = P.single_mode_problem(nt=nt, time_window_ps=10.0 if nt >= 1024 else 3.0, L=0.5,
                                power_w=0.1, rep_rate_hz=80.5e6, validate_grid=False)
     rng = np.random.default_rng(nt)
@@ -41,7 +42,38 @@ def test_rhs_matches_oracle(gpu_ctx, nt, precision):
     # forward RHS in the mode's precision; the adjoint RHS is FP64 in both modes
     tol = 2e-6 if precision == "fp32" else FIELD_TOL_FP64
     assert rel(gp.rhs(z, u), O.rhs_forward(fp, z, u)) < tol
-    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < FIELD_TOL_FP64
+    # The random λ fills every bin, and at the band edge the dispersion phase
+    # D(ω)z reaches ~7e6 rad on the 2^15 / 10 ps grid: one FP64 rounding of
+    # that argument is ~1e-9 rad, in the oracle as in the GPU.  Two FP64
+    # evaluations agree to about that floor, 2 eps max|D z|.
+    floor = 2 * np.finfo(float).eps * float(np.max(np.abs(fp.D))) * z
+    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < max(FIELD_TOL_FP64, floor)
+
+
+def test_forward_large_grids_against_tight_solution(gpu_ctx):
+    # Nt = 2^14 and 2^15 over 10 ps.  At the default tolerances (reltol 1e-8,
+    # abstol 1e-6) the RMS error norm is diluted over the mostly empty grid,
+    # and the oracle's own answer is 2e-5 (2^14) and 5e-5 (2^15) from the
+    # tight-tolerance solution; at 2^15 it moves by 1e-4 when reltol changes
+    # by one part in 10^7.  So the GPU solves are held against the tight
+    # solution (oracle, reltol = abstol = 1e-12), with bounds set by the
+    # oracle's own default-tolerance error there: FP64 mode within 3x of it;
+    # FP32 mode (whose FFT round-off floor enters the error norm in the empty
+    # bins and adds steps) within 10x.
+    for nt in (16384, 32768):
+        fp = P.single_mode_problem(nt=nt, time_window_ps=10.0, L=0.3, power_w=0.1,
+                                   rep_rate_hz=80.5e6, validate_grid=False)
+        ref, _, _ = O.forward(fp)
+        tight = P.FiberProblem(**{**fp.__dict__})
+        tight.reltol = tight.abstol = 1e-12
+        truth, _, _ = O.forward(tight)
+        e_ref = rel(ref[-1], truth[-1])
+        out64, _ = GPUProblem(gpu_ctx, fp, "fp64").forward() if nt == 32768 else (None, None)
+        out32, st = GPUProblem(gpu_ctx, fp).forward()
+        assert st["status"] == 0 and st["z_end"] == fp.L
+        assert rel(out32[-1], truth[-1]) < max(10 * e_ref, FIELD_TOL_FP32)
+        if out64 is not None:
+            assert rel(out64[-1], truth[-1]) < 3 * e_ref
 
 
 @pytest.mark.parametrize("nt,T", [(256, 3.0), (1024, 10.0), (2048, 10.0), (4096, 10.0)])
@@ -134,6 +166,23 @@ def test_band_gradient_config1(gpu_ctx, log_cost):
         assert abs(10 * np.log10(J[0]) - 10 * np.log10(Jo)) < DB_TOL
     assert rel(g[0], go) < GRAD_TOL
     assert st[0]["checkpoints_used"] <= 32
+
+
+def test_band_gradient_2p15(gpu_ctx):
+    # Nt = 2^15 over 10 ps (the serving mix's largest grid) through the
+    # cluster transform: forward, band objective, adjoint and gradient
+    # (0.1 m; phase N(0, 0.5²) windowed to the pulse band: a white phase at
+    # this grid spreads energy over ±1640 THz and the solves take thousands
+    # of steps in the oracle)
+    fp = P.single_mode_problem(nt=32768, time_window_ps=10.0, L=0.1, power_w=0.1,
+                               rep_rate_hz=80e6, validate_grid=False, raman_threshold_thz=-5.0)
+    f = P.fftfreq(fp.nt, 1 / fp.sim["Δt"])
+    phi = 0.5 * np.random.default_rng(15).standard_normal(fp.nt) * np.exp(-(f / 4.0) ** 2)
+    J, g, st = GPUProblem(gpu_ctx, fp).phase_gradient_batch(phi[None, :])
+    Jo, go, _ = O.phase_gradient(fp, phi)
+    assert abs(10 * np.log10(J[0]) - 10 * np.log10(Jo)) < DB_TOL
+    assert rel(g[0], go) < GRAD_TOL
+    assert st[0]["status"] == 0
 
 
 def test_gradient_central_differences(gpu_ctx):
