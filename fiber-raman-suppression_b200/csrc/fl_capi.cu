@@ -4,7 +4,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -191,23 +198,26 @@ char* carve(char*& p, size_t bytes) {
 
 // Allocate a workspace for B slots; descriptors point into it.  Caller
 // buffers (u0 etc.) are per-slot arrays inside the workspace.
-int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
+int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out,
+                const fl_ctx_opts* opt = nullptr, cudaStream_t stream = nullptr) {
     const size_t rf = pr->precision == FL_PRECISION_FP64 ? 8 : 4;
     fl_ctx* ctx = pr->ctx;
+    const fl_ctx_opts& o = opt ? *opt : ctx->opts;
+    cudaStream_t strm = opt ? stream : ctx->stream;
     auto w = std::make_unique<Work>();
     w->ctx = ctx;
     w->B = B;
     w->nt = pr->nt;
     w->rsize = (int)rf;
-    w->K = ctx->opts.checkpoints;
-    w->segcap = ctx->opts.segment_steps;
-    w->stepcap = ctx->opts.step_log;
+    w->K = o.checkpoints;
+    w->segcap = o.segment_steps;
+    w->stepcap = o.step_log;
     w->nsave = nsave;
     const int nt = pr->nt;
     const size_t per = slot_bytes(nt, rf, w->K, w->segcap, w->stepcap);
     const size_t io = 16 * (size_t)nt * (2 + nsave + 2) + 8 * (size_t)nt + 256 * 8;
     w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + nt + 4096;
-    if (ctx->opts.hbm_budget_bytes && w->pool_bytes > ctx->opts.hbm_budget_bytes)
+    if (o.hbm_budget_bytes && w->pool_bytes > o.hbm_budget_bytes)
         return set_err(ctx, FL_OOM_ADMISSION, "workspace of %zu bytes exceeds the HBM budget",
                        w->pool_bytes);
     CU(cudaMalloc(&w->pool, w->pool_bytes));
@@ -245,7 +255,7 @@ int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
         d.ck_cap = w->K;
         d.seg_cap = w->segcap;
         d.step_cap = w->stepcap;
-        d.max_iters = ctx->opts.max_iters;
+        d.max_iters = o.max_iters;
         d.zsave = w->d_zsave;
         d.save_out = nsave ? w->d_save + (size_t)b * 2 * nt * nsave : nullptr;
         d.u0 = w->d_u0 + (size_t)b * 2 * nt;
@@ -273,13 +283,13 @@ int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out) {
         return set_err(ctx, FL_ECUDA, "internal: workspace overflow (%zu > %zu)",
                        (size_t)(p - w->pool), w->pool_bytes);
     CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), w->h_desc.size(), cudaMemcpyHostToDevice,
-                       ctx->stream));
+                       strm));
     std::vector<int> act(B);
     for (int b = 0; b < B; b++) act[b] = b;
     CU(cudaMemcpyAsync(w->d_active, act.data(), sizeof(int) * B, cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState) * B, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
+                       strm));
+    CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState) * B, strm));
+    CU(cudaStreamSynchronize(strm));
     *out = w.release();
     return FL_OK;
 }
@@ -449,8 +459,11 @@ size_t mm_slot_bytes(size_t nm, size_t npn, size_t rf, int K, int segcap, int st
     return b + 40 * 256;                 // alignment of the carved buffers
 }
 
-int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmWork** out) {
+int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmWork** out,
+                   const fl_ctx_opts* opt = nullptr, cudaStream_t stream = nullptr) {
     fl_ctx* ctx = pr->ctx;
+    const fl_ctx_opts& o = opt ? *opt : ctx->opts;
+    cudaStream_t strm = opt ? stream : ctx->stream;
     const size_t rf = pr->precision == FL_PRECISION_FP64 ? 8 : 4;
     auto w = std::make_unique<MmWork>();
     w->ctx = ctx;
@@ -458,9 +471,9 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     w->nt = pr->nt;
     w->m = pr->m;
     w->np = pr->m * (pr->m + 1) / 2;
-    w->K = ctx->opts.checkpoints;
-    w->segcap = ctx->opts.segment_steps;
-    w->stepcap = ctx->opts.step_log;
+    w->K = o.checkpoints;
+    w->segcap = o.segment_steps;
+    w->stepcap = o.step_log;
     w->nsave = nsave;
     w->per_mode = per_mode;
     const size_t nm = (size_t)pr->nt * pr->m, npn = (size_t)w->np * pr->nt;
@@ -468,7 +481,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     const size_t per = mm_slot_bytes(nm, npn, rf, w->K, w->segcap, w->stepcap, nparts);
     const size_t io = 16 * nm * (4 + nsave) + 8 * nm + 256 * 8;
     w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + pr->nt + 4096;
-    if (ctx->opts.hbm_budget_bytes && w->pool_bytes > ctx->opts.hbm_budget_bytes)
+    if (o.hbm_budget_bytes && w->pool_bytes > o.hbm_budget_bytes)
         return set_err(ctx, FL_OOM_ADMISSION, "workspace of %zu bytes exceeds the HBM budget",
                        w->pool_bytes);
     CU(cudaMalloc(&w->pool, w->pool_bytes));
@@ -513,7 +526,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         d.ck_cap = w->K;
         d.seg_cap = w->segcap;
         d.step_cap = w->stepcap;
-        d.max_iters = ctx->opts.max_iters;
+        d.max_iters = o.max_iters;
         d.zsave = w->d_zsave;
         d.save_out = nsave ? w->d_save + (size_t)b * 2 * nm * nsave : nullptr;
         d.u0 = w->d_u0 + (size_t)b * 2 * nm;
@@ -544,13 +557,13 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         return set_err(ctx, FL_ECUDA, "internal: workspace overflow (%zu > %zu)",
                        (size_t)(p - w->pool), w->pool_bytes);
     CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), sizeof(MmDesc) * B, cudaMemcpyHostToDevice,
-                       ctx->stream));
+                       strm));
     std::vector<int> act(B);
     for (int b = 0; b < B; b++) act[b] = b;
     CU(cudaMemcpyAsync(w->d_active, act.data(), sizeof(int) * B, cudaMemcpyHostToDevice,
-                       ctx->stream));
-    CU(cudaMemsetAsync(w->d_state, 0, sizeof(MmState) * B, ctx->stream));
-    CU(cudaStreamSynchronize(ctx->stream));
+                       strm));
+    CU(cudaMemsetAsync(w->d_state, 0, sizeof(MmState) * B, strm));
+    CU(cudaStreamSynchronize(strm));
     *out = w.release();
     return FL_OK;
 }
@@ -804,6 +817,393 @@ int mm_phase_gradient_device(fl_problem* pr, const double* d_u0, int nbatch,
         if (st[b].status != ST_OK)
             return set_err(ctx, st[b].status, "slot %d: %s", b, fl_status_string(st[b].status));
     return FL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// serving runtime
+// ---------------------------------------------------------------------------
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+}  // namespace
+
+struct SrvRequest {
+    long id = 0;
+    fl_problem* prob = nullptr;
+    int kind = FL_REQ_FORWARD, log_cost = 0;
+    double L = 0;
+    std::vector<double> u0;            // shaped launch, (Nt, M) complex
+    std::vector<unsigned char> mask;
+    double* out_field = nullptr;
+    double* out_grad = nullptr;
+    int status = FL_EBUSY;
+    fl_stats stats{};
+    double J = 0, t_submit = 0, t_done = 0;
+};
+
+// One chunk of slots of one bucket, advanced on its own stream.
+struct SrvChunk {
+    bool mm = false;
+    Work* w = nullptr;
+    MmWork* mw = nullptr;
+    int B = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool inflight = false;
+    std::vector<SrvRequest*> slot;     // nullptr: free
+    unsigned char* d_masks = nullptr;  // per-slot band masks (B * Nt)
+    size_t bytes = 0;
+    std::vector<SlotState> hs;
+    std::vector<MmState> hms;
+    ~SrvChunk() {
+        delete w;
+        delete mw;
+        cudaFree(d_masks);
+        if (ev) cudaEventDestroy(ev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+// Requests of one shape (Nt, M, precision): slots of one chunk share the
+// kernel instance; each slot's descriptor points at its request's tables.
+struct SrvBucket {
+    int nt = 0, m = 0, precision = 0;
+    bool mm = false;
+    fl_problem* tables = nullptr;      // server-owned twiddles (and defaults) for free slots
+    std::vector<SrvChunk*> chunks;
+    std::deque<SrvRequest*> pending;
+    ~SrvBucket() {
+        for (auto* c : chunks) delete c;
+        if (tables) fl_problem_destroy(tables);
+    }
+};
+
+struct fl_server {
+    fl_ctx* ctx = nullptr;
+    fl_server_opts opts{};
+    fl_ctx_opts wopts{};
+    std::mutex mu;
+    std::condition_variable cv;
+    std::map<long, SrvRequest*> reqs;
+    std::deque<SrvRequest*> incoming;
+    std::vector<SrvBucket*> buckets;
+    size_t hbm_used = 0;
+    long next_id = 1, submitted = 0, completed = 0, launches = 0;
+    int fatal = FL_OK;
+    std::string err;
+    std::atomic<bool> stop{false};
+    std::thread th;
+};
+
+namespace {
+
+// slot footprint of one request of this shape, with the server's options
+size_t srv_slot_bytes(const fl_server* sv, const fl_problem* pr) {
+    const size_t rf = pr->precision == FL_PRECISION_FP64 ? 8 : 4;
+    const fl_ctx_opts& o = sv->wopts;
+    if (!pr->use_mm) return slot_bytes(pr->nt, rf, o.checkpoints, o.segment_steps, o.step_log) +
+                            16 * (size_t)pr->nt * 4 + 8 * (size_t)pr->nt + 2 * (size_t)pr->nt;
+    const size_t nm = (size_t)pr->nt * pr->m, np = (size_t)pr->m * (pr->m + 1) / 2;
+    return mm_slot_bytes(nm, np * pr->nt, rf, o.checkpoints, o.segment_steps, o.step_log,
+                         pr->m * mm_cluster_ctas(ilog2i(pr->nt))) +
+           16 * nm * 4 + 8 * nm + 2 * (size_t)pr->nt;
+}
+
+int srv_chunk_slots(const SrvBucket* b) {
+    if (!b->mm) return 148;
+    return std::max(1, 148 / (b->m * mm_cluster_ctas(ilog2i(b->nt))));
+}
+
+// a bucket's own table set: a problem with this shape's grid (zero tables),
+// so free slots always point at live twiddles
+int srv_bucket_tables(fl_server* sv, SrvBucket* b) {
+    const int nt = b->nt, m = b->m;
+    std::vector<double> D((size_t)nt * m, 0.0), g((size_t)m * m * m * m, 0.0), h(2 * (size_t)nt, 0.0),
+        ss(nt, 1.0);
+    for (int i = 0; i < m; i++) g[i + m * (i + m * (i + m * i))] = 1.0;
+    return fl_problem_create(sv->ctx, nt, m, D.data(), g.data(), h.data(), ss.data(), 1.0, 1.0,
+                             1e-8, 1e-6, b->precision, &b->tables);
+}
+
+int srv_new_chunk(fl_server* sv, SrvBucket* b) {
+    fl_ctx* ctx = sv->ctx;
+    auto c = std::make_unique<SrvChunk>();
+    c->mm = b->mm;
+    c->B = srv_chunk_slots(b);
+    const size_t need = srv_slot_bytes(sv, b->tables) * c->B;
+    if (sv->opts.hbm_budget_bytes && sv->hbm_used + need > sv->opts.hbm_budget_bytes) {
+        // a smaller chunk if at least one slot fits
+        const size_t one = srv_slot_bytes(sv, b->tables);
+        const size_t left = sv->opts.hbm_budget_bytes - std::min(sv->hbm_used, sv->opts.hbm_budget_bytes);
+        c->B = (int)std::min<size_t>(c->B, left / one);
+        if (c->B < 1) return FL_OOM_ADMISSION;
+    }
+    CU(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming));
+    fl_ctx_opts o = sv->wopts;
+    o.hbm_budget_bytes = 0;
+    int rc = c->mm ? mm_work_create(b->tables, c->B, 0, MODE_FORWARD, 0, &c->mw, &o, c->stream)
+                   : work_create(b->tables, c->B, 0, MODE_FORWARD, &c->w, &o, c->stream);
+    if (rc) return rc;
+    CU(cudaMalloc(&c->d_masks, (size_t)c->B * b->nt));
+    // every slot starts free (finished)
+    if (c->mm) {
+        std::vector<MmState> st(c->B);
+        for (auto& x : st) {
+            memset(&x, 0, sizeof x);
+            x.phase = PH_DONE;
+        }
+        CU(cudaMemcpyAsync(c->mw->d_state, st.data(), sizeof(MmState) * c->B,
+                           cudaMemcpyHostToDevice, c->stream));
+    } else {
+        std::vector<SlotState> st(c->B);
+        for (auto& x : st) {
+            memset(&x, 0, sizeof x);
+            x.phase = PH_DONE;
+        }
+        CU(cudaMemcpyAsync(c->w->d_state, st.data(), sizeof(SlotState) * c->B,
+                           cudaMemcpyHostToDevice, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    c->slot.assign(c->B, nullptr);
+    c->bytes = (c->mm ? c->mw->pool_bytes : c->w->pool_bytes) + (size_t)c->B * b->nt;
+    sv->hbm_used += c->bytes;
+    b->chunks.push_back(c.release());
+    return FL_OK;
+}
+
+// place request r into free slot i of chunk c (stream-ordered before the next launch)
+int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
+    fl_ctx* ctx = sv->ctx;
+    const fl_problem* pr = r->prob;
+    const size_t nm = (size_t)b->nt * b->m;
+    const int mode = r->kind == FL_REQ_BAND_GRADIENT ? MODE_BAND_GRADIENT : MODE_FORWARD;
+    unsigned char* dmask = c->d_masks + (size_t)i * b->nt;
+    if (!r->mask.empty())
+        CU(cudaMemcpyAsync(dmask, r->mask.data(), b->nt, cudaMemcpyHostToDevice, c->stream));
+    if (c->mm) {
+        MmDesc& d = c->mw->h_desc[i];
+        d.Dturns = pr->d_Dturns;
+        for (int q = 0; q < 2; q++) {
+            d.Heff[q] = pr->d_Heff[q];
+            d.ss[q] = pr->d_ss[q];
+            d.G[q] = pr->d_G[q];
+        }
+        d.one_m_fR = pr->one_m_fR;
+        d.L = r->L;
+        d.reltol = pr->reltol;
+        d.abstol = pr->abstol;
+        d.mode = mode;
+        d.log_cost = r->log_cost;
+        d.phase_per_mode = 0;
+        d.mask = dmask;
+        CU(cudaMemcpyAsync((double*)d.u0, r->u0.data(), 16 * nm, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaMemcpyAsync((MmDesc*)c->mw->d_desc + i, &d, sizeof(MmDesc), cudaMemcpyHostToDevice,
+                           c->stream));
+        CU(cudaMemsetAsync(c->mw->d_state + i, 0, sizeof(MmState), c->stream));
+    } else {
+        SlotDesc& d = reinterpret_cast<SlotDesc*>(c->w->h_desc.data())[i];
+        d.Dturns = pr->d_Dturns;
+        for (int q = 0; q < 2; q++) {
+            d.Heff[q] = pr->d_Heff[q];
+            d.ss[q] = pr->d_ss[q];
+        }
+        d.gamma = pr->gamma0;
+        d.one_m_fR = pr->one_m_fR;
+        d.L = r->L;
+        d.reltol = pr->reltol;
+        d.abstol = pr->abstol;
+        d.mode = mode;
+        d.log_cost = r->log_cost;
+        d.mask = dmask;
+        CU(cudaMemcpyAsync((double*)d.u0, r->u0.data(), 16 * nm, cudaMemcpyHostToDevice, c->stream));
+        CU(cudaMemcpyAsync((SlotDesc*)c->w->d_desc + i, &d, sizeof(SlotDesc), cudaMemcpyHostToDevice,
+                           c->stream));
+        CU(cudaMemsetAsync(c->w->d_state + i, 0, sizeof(SlotState), c->stream));
+    }
+    c->slot[i] = r;
+    return FL_OK;
+}
+
+// after a launch: copy finished requests' results out and free their slots
+// (the status is published under the server lock by the caller)
+int srv_retire(fl_server* sv, SrvBucket* b, SrvChunk* c,
+               std::vector<std::pair<SrvRequest*, int>>& done) {
+    fl_ctx* ctx = sv->ctx;
+    const size_t nm = (size_t)b->nt * b->m;
+    if (c->mm) {
+        c->hms.resize(c->B);
+        CU(cudaMemcpyAsync(c->hms.data(), c->mw->d_state, sizeof(MmState) * c->B,
+                           cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        c->hs.resize(c->B);
+        CU(cudaMemcpyAsync(c->hs.data(), c->w->d_state, sizeof(SlotState) * c->B,
+                           cudaMemcpyDeviceToHost, c->stream));
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < c->B; i++) {
+        SrvRequest* r = c->slot[i];
+        if (!r) continue;
+        const int ph = c->mm ? c->hms[i].phase : c->hs[i].phase;
+        if (ph != PH_DONE) continue;
+        int st;
+        if (c->mm) {
+            mm_fill_stats(c->hms[i], &r->stats);
+            st = c->hms[i].status;
+            r->J = c->hms[i].J;
+        } else {
+            fill_stats(c->hs[i], &r->stats);
+            st = c->hs[i].status;
+            r->J = c->hs[i].J;
+        }
+        if (st == ST_OK) {
+            const double* uL = c->mm ? c->mw->h_desc[i].uL_out
+                                     : reinterpret_cast<SlotDesc*>(c->w->h_desc.data())[i].uL_out;
+            const double* gr = c->mm ? c->mw->h_desc[i].grad_out
+                                     : reinterpret_cast<SlotDesc*>(c->w->h_desc.data())[i].grad_out;
+            if (r->kind == FL_REQ_FORWARD && r->out_field)
+                CU(cudaMemcpyAsync(r->out_field, uL, 16 * nm, cudaMemcpyDeviceToHost, c->stream));
+            if (r->kind == FL_REQ_BAND_GRADIENT && r->out_grad)
+                CU(cudaMemcpyAsync(r->out_grad, gr, 8 * (size_t)b->nt, cudaMemcpyDeviceToHost,
+                                   c->stream));
+        }
+        c->slot[i] = nullptr;
+        done.emplace_back(r, st);
+    }
+    CU(cudaStreamSynchronize(c->stream));
+    return FL_OK;
+}
+
+int srv_launch(fl_server* sv, SrvBucket* b, SrvChunk* c) {
+    fl_ctx* ctx = sv->ctx;
+    const int logn = ilog2i(b->nt);
+    if (c->mm) {
+        MmRound a{};
+        a.desc = c->mw->d_desc;
+        a.state = c->mw->d_state;
+        a.active = c->mw->d_active;
+        a.nactive = c->B;
+        a.M = b->m;
+        a.NP = c->mw->np;
+        a.N = b->nt;
+        a.fp64 = b->precision == FL_PRECISION_FP64;
+        a.control = 1;
+        a.ndone = nullptr;
+        a.stream = c->stream;
+        MmRoundFn round = mm_round_launcher(logn);
+        CU(mm_launch_control(a, 0));  // prepares newly admitted slots (idempotent for the rest)
+        for (int r = 0; r < sv->opts.evals_per_launch; r++) CU(round(a));
+        sv->launches += 1 + (long)sv->opts.evals_per_launch * (a.fp64 ? 7 : 10);
+    } else {
+        LaunchFn fn = sm_launcher(b->precision == FL_PRECISION_FP64, logn);
+        LaunchArgs a{c->w->d_desc, c->w->d_state, c->w->d_active, c->B,
+                     sv->opts.evals_per_launch, c->stream};
+        CU(fn(a));
+        sv->launches++;
+    }
+    CU(cudaEventRecord(c->ev, c->stream));
+    c->inflight = true;
+    return FL_OK;
+}
+
+SrvBucket* srv_bucket_for(fl_server* sv, const fl_problem* pr) {
+    for (auto* b : sv->buckets)
+        if (b->nt == pr->nt && b->m == pr->m && b->precision == pr->precision) return b;
+    return nullptr;
+}
+
+// One pass over every bucket; returns whether anything happened.
+int srv_progress(fl_server* sv, bool& did) {
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        while (!sv->incoming.empty()) {
+            SrvRequest* r = sv->incoming.front();
+            sv->incoming.pop_front();
+            SrvBucket* b = srv_bucket_for(sv, r->prob);
+            if (!b) {
+                b = new SrvBucket();
+                b->nt = r->prob->nt;
+                b->m = r->prob->m;
+                b->precision = r->prob->precision;
+                b->mm = r->prob->use_mm;
+                sv->buckets.push_back(b);
+                int rc = srv_bucket_tables(sv, b);
+                if (rc) return rc;
+            }
+            b->pending.push_back(r);
+            did = true;
+        }
+    }
+    std::vector<std::pair<SrvRequest*, int>> done;
+    for (auto* b : sv->buckets) {
+        for (auto* c : b->chunks) {
+            if (c->inflight) {
+                const cudaError_t q = cudaEventQuery(c->ev);
+                if (q == cudaErrorNotReady) continue;
+                if (q != cudaSuccess) {
+                    fl_ctx* ctx = sv->ctx;
+                    CU(q);
+                }
+                c->inflight = false;
+                int rc = srv_retire(sv, b, c, done);
+                if (rc) return rc;
+                did = true;
+            }
+            for (int i = 0; i < c->B && !b->pending.empty(); i++)
+                if (!c->slot[i]) {
+                    int rc = srv_admit(sv, b, c, i, b->pending.front());
+                    if (rc) return rc;
+                    b->pending.pop_front();
+                    did = true;
+                }
+            bool any = false;
+            for (auto* r : c->slot) any |= r != nullptr;
+            if (any) {
+                int rc = srv_launch(sv, b, c);
+                if (rc) return rc;
+                did = true;
+            }
+        }
+        // grow while requests wait and the budget allows
+        if (!b->pending.empty()) {
+            const int rc = srv_new_chunk(sv, b);
+            if (rc == FL_OK) did = true;
+            else if (rc != FL_OOM_ADMISSION) return rc;
+        }
+    }
+    if (!done.empty()) {
+        const double t = now_ms();
+        std::lock_guard<std::mutex> lk(sv->mu);
+        for (auto& rs : done) {
+            rs.first->t_done = t;
+            rs.first->status = rs.second;
+            sv->completed++;
+        }
+        sv->cv.notify_all();
+    }
+    return FL_OK;
+}
+
+void srv_thread(fl_server* sv) {
+    cudaSetDevice(sv->ctx->device);
+    while (!sv->stop.load()) {
+        bool did = false;
+        const int rc = srv_progress(sv, did);
+        if (rc) {
+            std::lock_guard<std::mutex> lk(sv->mu);
+            sv->fatal = rc;
+            sv->err = sv->ctx->err;
+            for (auto& kv : sv->reqs)
+                if (kv.second->status == FL_EBUSY) kv.second->status = rc;
+            sv->cv.notify_all();
+            return;
+        }
+        if (!did) std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
 }
 
 }  // namespace
@@ -1241,6 +1641,168 @@ int fl_mode_phase_gradient_batch(fl_problem* pr, const double* u0, int nbatch,
                                  double* J, double* grad, fl_stats* stats) {
     return phase_gradient_host(pr, u0, nbatch, phases, pr && pr->m > 1 ? 1 : 0, mask, log_cost,
                                J, grad, stats);
+}
+
+int fl_server_create(fl_ctx* ctx, const fl_server_opts* opts, fl_server** out) {
+    if (!ctx || !out) return FL_EINVAL;
+    *out = nullptr;
+    auto sv = std::make_unique<fl_server>();
+    sv->ctx = ctx;
+    sv->opts.hbm_budget_bytes = (size_t)120 << 30;
+    sv->opts.evals_per_launch = 48;
+    sv->opts.checkpoints = 64;
+    sv->opts.segment_steps = 128;
+    if (opts) {
+        if (opts->hbm_budget_bytes) sv->opts.hbm_budget_bytes = opts->hbm_budget_bytes;
+        if (opts->evals_per_launch > 0) sv->opts.evals_per_launch = opts->evals_per_launch;
+        if (opts->checkpoints > 0) sv->opts.checkpoints = opts->checkpoints;
+        if (opts->segment_steps > 0) sv->opts.segment_steps = opts->segment_steps;
+    }
+    if (!pow2(sv->opts.checkpoints) || sv->opts.checkpoints < 2)
+        return set_err(ctx, FL_EINVAL, "server checkpoints must be a power of two >= 2");
+    sv->wopts = ctx->opts;
+    sv->wopts.checkpoints = sv->opts.checkpoints;
+    sv->wopts.segment_steps = sv->opts.segment_steps;
+    sv->wopts.step_log = std::max(ctx->opts.step_log,
+                                  sv->opts.checkpoints * sv->opts.segment_steps);
+    fl_server* p = sv.release();
+    p->th = std::thread(srv_thread, p);
+    *out = p;
+    return FL_OK;
+}
+
+int fl_server_destroy(fl_server* sv) {
+    if (!sv) return FL_EINVAL;
+    sv->stop.store(true);
+    if (sv->th.joinable()) sv->th.join();
+    cudaSetDevice(sv->ctx->device);
+    for (auto* b : sv->buckets) {
+        for (auto* c : b->chunks)
+            if (c->stream) cudaStreamSynchronize(c->stream);
+        delete b;
+    }
+    // every request not yet handed back is in reqs (queued, running or finished)
+    for (auto& kv : sv->reqs) delete kv.second;
+    delete sv;
+    return FL_OK;
+}
+
+int fl_server_submit(fl_server* sv, const fl_request* q, long* id) {
+    if (!sv || !q || !id || !q->prob || !q->u0) return FL_EINVAL;
+    fl_ctx* ctx = sv->ctx;
+    fl_problem* pr = q->prob;
+    if (q->kind != FL_REQ_FORWARD && q->kind != FL_REQ_BAND_GRADIENT)
+        return set_err(ctx, FL_EINVAL, "unknown request kind %d", q->kind);
+    if (q->kind == FL_REQ_BAND_GRADIENT) {
+        if (!q->phase || !q->mask || !q->out_grad)
+            return set_err(ctx, FL_EINVAL, "band-gradient request needs phase, mask and out_grad");
+        if (!pr->gamma_sym)
+            return set_err(ctx, FL_NONSYMMETRIC,
+                           "fiber adjoint requires a fully permutation-symmetric gamma tensor");
+    } else if (!q->out_field) {
+        return set_err(ctx, FL_EINVAL, "forward request needs out_field");
+    }
+    const int logn = ilog2i(pr->nt);
+    if (pr->use_mm ? !mm_round_launcher(logn)
+                   : !sm_launcher(pr->precision == FL_PRECISION_FP64, logn))
+        return set_err(ctx, FL_EUNSUPPORTED, "shape not built (Nt = %d, M = %d)", pr->nt, pr->m);
+    const size_t one = srv_slot_bytes(sv, pr) * 1;
+    if (sv->opts.hbm_budget_bytes && one > sv->opts.hbm_budget_bytes)
+        return set_err(ctx, FL_OOM_ADMISSION, "one slot of %zu bytes exceeds the HBM budget", one);
+    const double L = q->L > 0 ? q->L : pr->L;
+    if (!std::isfinite(L)) return set_err(ctx, FL_EINVAL, "L must be positive and finite");
+    auto r = std::make_unique<SrvRequest>();
+    r->prob = pr;
+    r->kind = q->kind;
+    r->log_cost = q->log_cost;
+    r->L = L;
+    const size_t nm = (size_t)pr->nt * pr->m;
+    r->u0.assign(q->u0, q->u0 + 2 * nm);
+    double nrm = 0.0;
+    for (double x : r->u0) {
+        if (!std::isfinite(x)) return set_err(ctx, FL_EINVAL, "input spectrum must be finite");
+        nrm += x * x;
+    }
+    if (!(nrm > 0)) return set_err(ctx, FL_EINVAL, "input spectrum must be nonzero");
+    if (q->kind == FL_REQ_BAND_GRADIENT) {
+        bool any = false;
+        r->mask.assign(q->mask, q->mask + pr->nt);
+        for (auto x : r->mask) any |= x != 0;
+        if (!any) return set_err(ctx, FL_EINVAL, "band mask must contain at least one bin");
+        // u_shaped = u0 ⊙ cis(φ) (physics_models.jl:791-797)
+        for (size_t k = 0; k < nm; k++) {
+            const double ph = q->phase[k % pr->nt];
+            if (!std::isfinite(ph)) return set_err(ctx, FL_EINVAL, "phase values must be finite");
+            const double c = std::cos(ph), s = std::sin(ph), a = r->u0[2 * k], b = r->u0[2 * k + 1];
+            r->u0[2 * k] = a * c - b * s;
+            r->u0[2 * k + 1] = a * s + b * c;
+        }
+        r->out_grad = q->out_grad;
+    } else {
+        r->out_field = q->out_field;
+    }
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (sv->fatal) return set_err(ctx, sv->fatal, "server stopped: %s", sv->err.c_str());
+    r->id = sv->next_id++;
+    r->t_submit = now_ms();
+    *id = r->id;
+    sv->reqs[r->id] = r.get();
+    sv->incoming.push_back(r.release());
+    sv->submitted++;
+    return FL_OK;
+}
+
+static int srv_result(fl_server* sv, SrvRequest* r, fl_stats* stats, double* J, double* lat) {
+    if (stats) *stats = r->stats;
+    if (J) *J = r->J;
+    if (lat) *lat = r->t_done - r->t_submit;
+    const int st = r->status;
+    sv->reqs.erase(r->id);
+    delete r;
+    return st;
+}
+
+int fl_server_poll(fl_server* sv, long id, fl_stats* stats, double* J, double* latency_ms) {
+    if (!sv) return FL_EINVAL;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(id);
+    if (it == sv->reqs.end()) return FL_EINVAL;
+    if (it->second->status == FL_EBUSY) return FL_EBUSY;
+    return srv_result(sv, it->second, stats, J, latency_ms);
+}
+
+int fl_server_wait(fl_server* sv, long id, double timeout_ms, fl_stats* stats, double* J,
+                   double* latency_ms) {
+    if (!sv) return FL_EINVAL;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    auto it = sv->reqs.find(id);
+    if (it == sv->reqs.end()) return FL_EINVAL;
+    SrvRequest* r = it->second;
+    const auto until = std::chrono::steady_clock::now() +
+                       std::chrono::microseconds((long)(std::max(0.0, timeout_ms) * 1000));
+    while (r->status == FL_EBUSY)
+        if (sv->cv.wait_until(lk, until) == std::cv_status::timeout && r->status == FL_EBUSY)
+            return FL_TIMEOUT;
+    return srv_result(sv, r, stats, J, latency_ms);
+}
+
+int fl_server_info_get(fl_server* sv, fl_server_info* info) {
+    if (!sv || !info) return FL_EINVAL;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    info->submitted = sv->submitted;
+    info->completed = sv->completed;
+    info->queued = (long)sv->incoming.size();
+    info->in_flight = sv->submitted - sv->completed;
+    int slots = 0, chunks = 0;
+    for (auto* b : sv->buckets) {
+        chunks += (int)b->chunks.size();
+        for (auto* c : b->chunks) slots += c->B;
+    }
+    info->slots = slots;
+    info->chunks = chunks;
+    info->hbm_bytes = sv->hbm_used;
+    info->launches = sv->launches;
+    return FL_OK;
 }
 
 }  // extern "C"

@@ -26,7 +26,8 @@ EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_problem_destroy", "fl_forward", "fl_adjoint", "fl_phase_gradient_batch",
            "fl_phase_gradient_batch_device", "fl_rhs_eval", "fl_ctx_timing",
            "fl_forward_noalloc", "fl_mode_phase_gradient_batch",
-           "fl_mode_phase_gradient_batch_device")
+           "fl_mode_phase_gradient_batch_device", "fl_server_create", "fl_server_destroy",
+           "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_info_get")
 
 
 class FlCtxOpts(C.Structure):
@@ -39,6 +40,26 @@ class FlStats(C.Structure):
                 ("adj_naccept", C.c_long), ("adj_nreject", C.c_long), ("adj_nf", C.c_long),
                 ("status", C.c_int), ("checkpoints_used", C.c_int), ("J", C.c_double),
                 ("z_end", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class FlServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("evals_per_launch", C.c_int),
+                ("checkpoints", C.c_int), ("segment_steps", C.c_int)]
+
+
+class FlRequest(C.Structure):
+    _fields_ = [("prob", C.c_void_p), ("kind", C.c_int), ("L", C.c_double), ("u0", C.c_void_p),
+                ("phase", C.c_void_p), ("mask", C.c_void_p), ("log_cost", C.c_int),
+                ("out_field", C.c_void_p), ("out_grad", C.c_void_p)]
+
+
+class FlServerInfo(C.Structure):
+    _fields_ = [("submitted", C.c_long), ("completed", C.c_long), ("in_flight", C.c_long),
+                ("queued", C.c_long), ("slots", C.c_int), ("chunks", C.c_int),
+                ("hbm_bytes", C.c_size_t), ("launches", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -83,6 +104,14 @@ def load() -> C.CDLL:
         lib.fl_mode_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_rhs_eval.argtypes = [vp, ip, dp, vp, vp, vp]
         lib.fl_ctx_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.fl_server_create.argtypes = [vp, C.POINTER(FlServerOpts), C.POINTER(vp)]
+        lib.fl_server_destroy.argtypes = [vp]
+        lib.fl_server_submit.argtypes = [vp, C.POINTER(FlRequest), C.POINTER(C.c_long)]
+        lib.fl_server_poll.argtypes = [vp, C.c_long, C.POINTER(FlStats), C.POINTER(C.c_double),
+                                       C.POINTER(C.c_double)]
+        lib.fl_server_wait.argtypes = [vp, C.c_long, C.c_double, C.POINTER(FlStats),
+                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.fl_server_info_get.argtypes = [vp, C.POINTER(FlServerInfo)]
         lib.fl_forward_noalloc.argtypes = [ip, ip, vp, dp, vp, vp, dp, dp, dp, dp, vp, vp, ip,
                                            vp, vp, C.POINTER(FlStats)]
         _lib = lib

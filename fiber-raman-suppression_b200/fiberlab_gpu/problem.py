@@ -400,3 +400,50 @@ def centroid_thz(spectrum: np.ndarray, sim: dict) -> float:
     f = fftfreq(sim["Nt"], 1 / sim["Δt"])
     e = np.sum(np.abs(spectrum) ** 2, axis=0)
     return float(np.sum(f * e) / np.sum(e))
+
+
+# ---------------------------------------------------------------------------
+# Serving request mix (synthetic, seeded)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class ServeRequest:
+    arrival_s: float
+    nt: int
+    L: float
+    power_w: float
+    kind: int            # 0 forward, 1 forward + band gradient
+    phase: Optional[np.ndarray] = None
+
+
+def serving_grid_problem(nt: int, time_window_ps: float = 10.0) -> FiberProblem:
+    """The per-grid tables of the serving mix: SMF-28, 185 fs sech² at
+    80 MHz, band < -13 THz (lengths and powers vary per request)."""
+    return single_mode_problem(nt=nt, time_window_ps=time_window_ps, L=1.0, power_w=0.1,
+                               rep_rate_hz=80e6, raman_threshold_thz=-13.0,
+                               validate_grid=False)
+
+
+def serving_launch(fp: FiberProblem, power_w: float) -> np.ndarray:
+    """Launch spectrum of the serving grid at an average power (the sech²
+    pulse of get_initial_state scaled to P_avg)."""
+    return fp.uw0 * math.sqrt(power_w / 0.1)
+
+
+def serving_mix(n: int, seed: int = 0, rate_hz: float = 2000.0, log2_nt=(11, 15),
+                L_range=(0.1, 5.0), p_range=(0.02, 0.3)) -> list:
+    """n requests with exponential inter-arrival gaps (Poisson arrivals at
+    rate_hz), log2 Nt uniform on log2_nt, L ~ U(L_range) m, P ~ U(p_range) W,
+    half forward-only and half forward + band gradient with a launch phase
+    N(0, 0.5²) per bin."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate_hz, n))
+    out = []
+    for i in range(n):
+        nt = 1 << int(rng.integers(log2_nt[0], log2_nt[1] + 1))
+        L = float(rng.uniform(*L_range))
+        P = float(rng.uniform(*p_range))
+        kind = int(rng.integers(0, 2))
+        ph = 0.5 * rng.standard_normal(nt) if kind == 1 else None
+        out.append(ServeRequest(float(t[i]), nt, L, P, kind, ph))
+    return out

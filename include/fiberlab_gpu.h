@@ -191,6 +191,64 @@ int fl_forward_noalloc(int device, int nt, const double *d_D, double gamma, cons
                        double abstol, const double *d_u0, const double *d_saveat, int nsave,
                        double *d_out_spectra, void *stream, fl_stats *stats);
 
+/* ------------------------------------------------------------------------
+ * Serving: continuous batching of independent solves.  No counterpart in the
+ * reference (which solves one problem per call); it serves the request
+ * streams of the reference's callers (propagate / the adjoint model's
+ * physical gradient, physics_models.jl:1033-1046) without changing the
+ * per-solve arithmetic: each request runs the same stepper as fl_forward /
+ * fl_phase_gradient_batch, alone in its slot.
+ *
+ * A server owns a progress thread.  Requests are grouped by shape (Nt, M,
+ * precision) into buckets of slots; each chunk of slots is advanced by a
+ * bounded number of right-hand-side evaluations per launch on its own
+ * stream, and between launches finished slots are retired (results copied
+ * to the caller's buffers) and queued requests admitted into free slots.
+ * New chunks are allocated while the HBM budget allows.  All server calls
+ * are thread-safe.  Problems referenced by requests must outlive them.
+ * ------------------------------------------------------------------------ */
+#define FL_REQ_FORWARD 0        /* output: lab-frame field at L */
+#define FL_REQ_BAND_GRADIENT 1  /* outputs: Raman-band J and ∂J/∂φ */
+
+typedef struct {
+    size_t hbm_budget_bytes;  /* slot workspaces (default 120 GB) */
+    int evals_per_launch;     /* RHS evaluations per slot per launch (default 48) */
+    int checkpoints;          /* per-slot z-checkpoints (power of 2, default 64) */
+    int segment_steps;        /* recompute segment length (default 128) */
+} fl_server_opts;
+
+typedef struct {
+    fl_problem *prob;         /* tables, grid, tolerances */
+    int kind;                 /* FL_REQ_FORWARD or FL_REQ_BAND_GRADIENT */
+    double L;                 /* fiber length of this request; <= 0: the problem's */
+    const double *u0;         /* (Nt, M) complex launch spectrum, copied at submit */
+    const double *phase;      /* band gradient: Nt launch phase (shared by modes), copied */
+    const unsigned char *mask;/* band gradient: Nt band mask, copied */
+    int log_cost;
+    double *out_field;        /* forward: (Nt, M) complex lab field at L, written on completion */
+    double *out_grad;         /* band gradient: Nt, written on completion */
+} fl_request;
+
+typedef struct {
+    long submitted, completed, in_flight, queued;
+    int slots, chunks;
+    size_t hbm_bytes;         /* workspace bytes allocated */
+    long launches;
+} fl_server_info;
+
+int fl_server_create(fl_ctx *ctx, const fl_server_opts *opts, fl_server **out);
+int fl_server_destroy(fl_server *srv);
+/* Queue one request; returns its id.  FL_OOM_ADMISSION when one slot of its
+ * shape exceeds the HBM budget, FL_EUNSUPPORTED for shapes not built. */
+int fl_server_submit(fl_server *srv, const fl_request *req, long *id);
+/* FL_EBUSY while running; otherwise the request's final status (its
+ * outputs are written) with its stats, J and submit-to-completion latency. */
+int fl_server_poll(fl_server *srv, long id, fl_stats *stats, double *J, double *latency_ms);
+/* Block until done or timeout_ms elapses (FL_TIMEOUT). */
+int fl_server_wait(fl_server *srv, long id, double timeout_ms, fl_stats *stats, double *J,
+                   double *latency_ms);
+int fl_server_info_get(fl_server *srv, fl_server_info *info);
+
 #ifdef __cplusplus
 }
 #endif
