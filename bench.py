@@ -140,6 +140,91 @@ def cpu_baseline(fp, nthreads: int, nprob: int):
     return nprob / dt, dt
 
 
+def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
+    """Config-3 stream: n requests with Poisson arrivals at 2000/s, log2 Nt
+    uniform on 11..15 over 10 ps, L ~ U(0.1, 5) m, P ~ U(0.02, 0.3) W, half
+    forward-only and half forward + band gradient with phase N(0, 0.5²),
+    through the continuous-batching server; then the first plain_n requests
+    of the same stream one at a time through the plain entry points (a
+    problem per request, as the reference builds its tables per solve)."""
+    from fiberlab_gpu import problem as P
+    from fiberlab_gpu._capi import FiberLabGPUError, GPUProblem
+    from fiberlab_gpu.serving import Server
+    ctx = ctx_cls(dev_index)
+    reqs = P.serving_mix(n, seed=seed)
+    grids = {}
+    for r in reqs:
+        if r.nt not in grids:
+            fp = P.serving_grid_problem(r.nt)
+            grids[r.nt] = (fp, GPUProblem(ctx, fp))
+    srv = Server(ctx)
+    # allocate each shape's first chunk outside the measured stream
+    for nt, (fp, gp) in sorted(grids.items()):
+        srv.wait(srv.submit_forward(gp, u0=P.serving_launch(fp, 0.02), L=1e-3))
+    handles, statuses, lat = [], {}, []
+    t0 = time.perf_counter()
+    i, outstanding, t_last = 0, [], t0
+    while i < n or outstanding:
+        now = time.perf_counter() - t0
+        while i < n and reqs[i].arrival_s <= now:
+            r = reqs[i]
+            fp, gp = grids[r.nt]
+            u0 = P.serving_launch(fp, r.power_w)
+            h = (srv.submit_forward(gp, u0=u0, L=r.L) if r.kind == 0 else
+                 srv.submit_band_gradient(gp, r.phase, u0=u0, L=r.L))
+            outstanding.append(h)
+            i += 1
+        still = []
+        for h in outstanding:
+            try:
+                if not srv.poll(h):
+                    still.append(h)
+                    continue
+                statuses[0] = statuses.get(0, 0) + 1
+                lat.append(h.latency_ms)
+            except FiberLabGPUError as e:
+                statuses[e.status] = statuses.get(e.status, 0) + 1
+            t_last = time.perf_counter()
+        outstanding = still
+        time.sleep(0.0005)
+    wall = t_last - t0
+    info = srv.info()
+    srv.close()
+    done = statuses.get(0, 0)
+    out = {"requests": n, "completed": done,
+           "failed_by_status": {str(k): v for k, v in statuses.items() if k != 0},
+           "solves_per_s": done / wall, "wall_s": wall,
+           "latency_ms_p50": float(np.percentile(lat, 50)) if lat else None,
+           "latency_ms_p99": float(np.percentile(lat, 99)) if lat else None,
+           "slots": info["slots"], "hbm_bytes": info["hbm_bytes"],
+           "mix": "config 3: Poisson 2000/s, Nt 2^11..2^15 over 10 ps, L U(0.1,5) m, "
+                  "P U(0.02,0.3) W, half fwd / half fwd+adjoint (phase N(0,0.5^2)), FP32, seed 3"}
+    # plain one-at-a-time drop-in on the first plain_n requests of the stream
+    pctx = ctx_cls(dev_index, checkpoints=256, segment_steps=128, step_log=32768,
+                   max_iters=400000)
+    tp, pdone = 0.0, 0
+    for r in reqs[:plain_n]:
+        fp0, _ = grids[r.nt]
+        u0 = P.serving_launch(fp0, r.power_w)
+        t = time.perf_counter()
+        try:
+            fp = P.FiberProblem(**{**fp0.__dict__})
+            fp.L = r.L
+            gp = GPUProblem(pctx, fp)
+            if r.kind == 0:
+                gp.forward(u0)
+            else:
+                gp.phase_gradient_batch(r.phase[None, :], u0=u0)
+            pdone += 1
+        except FiberLabGPUError:
+            pass
+        tp += time.perf_counter() - t
+    out["plain_one_at_a_time"] = {"requests": plain_n, "completed": pdone,
+                                  "solves_per_s": plain_n / tp, "total_s": tp}
+    out["speedup_vs_plain"] = out["solves_per_s"] / out["plain_one_at_a_time"]["solves_per_s"]
+    return out
+
+
 def init_dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -278,6 +363,10 @@ def run_ours(args):
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{cores} problems of this workload, one per thread ({dt:.1f} s)"}
 
+    serving = None
+    if args.serve and rank == 0:
+        serving = serving_measure(Context, local, args.serve, args.serve_plain)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
@@ -294,6 +383,8 @@ def run_ours(args):
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
                 "plain_one_at_a_time": plain, "batched": batched_lat,
                 "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B}}
+        if serving is not None:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.destroy_process_group()
@@ -308,6 +399,10 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="problems per GPU (default 4 x SMs)")
     ap.add_argument("--plain", type=int, default=8, help="one-at-a-time solves timed")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve", type=int, default=0,
+                    help="also run the config-3 serving stream with this many requests")
+    ap.add_argument("--serve-plain", type=int, default=12,
+                    help="requests of that stream timed one at a time through the plain path")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -1344,7 +1344,9 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
     pr->abstol = abstol;
     pr->gamma0 = gamma[0];
     pr->gamma_sym = gamma_symmetric(gamma, m);
-    pr->use_mm = m > 1 || ilog2i(nt) > 14;
+    // the single-CTA stepper covers M = 1 up to 2^14 (FP32 mode) / 2^13 (FP64
+    // mode); larger transforms run on the multimode runtime's kernels
+    pr->use_mm = m > 1 || ilog2i(nt) > (precision == FL_PRECISION_FP64 ? 13 : 14);
     if (pr->use_mm && ((m > 1 && !mm_supported_modes(m)) || !mm_round_launcher(ilog2i(nt))))
         return set_err(ctx, FL_EUNSUPPORTED, "built shapes: M = 1 with Nt = 2^6..2^15, "
                        "M = 2..10 with Nt = 2^6..2^15 (got M = %d, Nt = %d)", m, nt);
@@ -1650,7 +1652,7 @@ int fl_server_create(fl_ctx* ctx, const fl_server_opts* opts, fl_server** out) {
     sv->ctx = ctx;
     sv->opts.hbm_budget_bytes = (size_t)120 << 30;
     sv->opts.evals_per_launch = 48;
-    sv->opts.checkpoints = 64;
+    sv->opts.checkpoints = 256;
     sv->opts.segment_steps = 128;
     if (opts) {
         if (opts->hbm_budget_bytes) sv->opts.hbm_budget_bytes = opts->hbm_budget_bytes;
@@ -1665,6 +1667,7 @@ int fl_server_create(fl_ctx* ctx, const fl_server_opts* opts, fl_server** out) {
     sv->wopts.segment_steps = sv->opts.segment_steps;
     sv->wopts.step_log = std::max(ctx->opts.step_log,
                                   sv->opts.checkpoints * sv->opts.segment_steps);
+    sv->wopts.max_iters = std::max(ctx->opts.max_iters, 400000L);
     fl_server* p = sv.release();
     p->th = std::thread(srv_thread, p);
     *out = p;

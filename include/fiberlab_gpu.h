@@ -213,8 +213,10 @@ int fl_forward_noalloc(int device, int nt, const double *d_D, double gamma, cons
 typedef struct {
     size_t hbm_budget_bytes;  /* slot workspaces (default 120 GB) */
     int evals_per_launch;     /* RHS evaluations per slot per launch (default 48) */
-    int checkpoints;          /* per-slot z-checkpoints (power of 2, default 64) */
-    int segment_steps;        /* recompute segment length (default 128) */
+    int checkpoints;          /* per-slot z-checkpoints (power of 2, default 256) */
+    int segment_steps;        /* recompute segment length (default 128); a band-gradient
+                                 request holds up to checkpoints x segment_steps accepted
+                                 forward steps (FL_ECAPACITY beyond) */
 } fl_server_opts;
 
 typedef struct {
