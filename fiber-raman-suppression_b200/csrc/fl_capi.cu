@@ -1001,6 +1001,9 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
         d.log_cost = r->log_cost;
         d.phase_per_mode = 0;
         d.mask = dmask;
+        // a forward-only request keeps no checkpoints or step log
+        d.ck_cap = mode == MODE_FORWARD ? 0 : c->mw->K;
+        d.step_cap = mode == MODE_FORWARD ? 0 : c->mw->stepcap;
         CU(cudaMemcpyAsync((double*)d.u0, r->u0.data(), 16 * nm, cudaMemcpyHostToDevice, c->stream));
         CU(cudaMemcpyAsync((MmDesc*)c->mw->d_desc + i, &d, sizeof(MmDesc), cudaMemcpyHostToDevice,
                            c->stream));
@@ -1020,6 +1023,9 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
         d.mode = mode;
         d.log_cost = r->log_cost;
         d.mask = dmask;
+        // a forward-only request keeps no checkpoints or step log
+        d.ck_cap = mode == MODE_FORWARD ? 0 : c->w->K;
+        d.step_cap = mode == MODE_FORWARD ? 0 : c->w->stepcap;
         CU(cudaMemcpyAsync((double*)d.u0, r->u0.data(), 16 * nm, cudaMemcpyHostToDevice, c->stream));
         CU(cudaMemcpyAsync((SlotDesc*)c->w->d_desc + i, &d, sizeof(SlotDesc), cudaMemcpyHostToDevice,
                            c->stream));

@@ -763,14 +763,16 @@ struct MmCtl {
                 return;
             }
             st.naccept++;
-            if (st.nsteps >= d.step_cap) {
-                st.status = ST_CAPACITY;
-                st.phase = PH_DONE;
-                return;
-            }
-            if (threadIdx.x == 0) {
-                d.steplog[2 * st.nsteps] = z;
-                d.steplog[2 * st.nsteps + 1] = dt;
+            if (d.step_cap > 0) {  // step_cap 0: forward only, nothing kept for an adjoint
+                if (st.nsteps >= d.step_cap) {
+                    st.status = ST_CAPACITY;
+                    st.phase = PH_DONE;
+                    return;
+                }
+                if (threadIdx.x == 0) {
+                    d.steplog[2 * st.nsteps] = z;
+                    d.steplog[2 * st.nsteps + 1] = dt;
+                }
             }
             double znew = z + dt;
             if (fabs(znew - d.L) < 100.0 * kEps * fmax(z, d.L)) znew = d.L;

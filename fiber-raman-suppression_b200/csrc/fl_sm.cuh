@@ -913,14 +913,16 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 continue;
             }
             st.naccept++;
-            if (st.nsteps >= d.step_cap) {
-                st.status = ST_CAPACITY;
-                st.phase = PH_DONE;
-                continue;
-            }
-            if (tid == 0) {
-                d.steplog[2 * st.nsteps] = z;
-                d.steplog[2 * st.nsteps + 1] = dt;
+            if (d.step_cap > 0) {  // step_cap 0: forward only, nothing kept for an adjoint
+                if (st.nsteps >= d.step_cap) {
+                    st.status = ST_CAPACITY;
+                    st.phase = PH_DONE;
+                    continue;
+                }
+                if (tid == 0) {
+                    d.steplog[2 * st.nsteps] = z;
+                    d.steplog[2 * st.nsteps + 1] = dt;
+                }
             }
             double znew = z + dt;
             if (fabs(znew - L) < 100.0 * kEps * fmax(z, L)) znew = L;  // snap to the tstop
