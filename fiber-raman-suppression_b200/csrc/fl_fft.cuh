@@ -293,6 +293,58 @@ __device__ __forceinline__ void gather_negated(const cx<R> (&v)[1 << LOGE], cx<R
     }
 }
 
+// Split the spectrum X of two packed real sequences p + i q and apply
+// v <- H P̂ + i conj(H) Q̂ in place, using X[k] and conj(X[-k]) read from
+// shared memory one bin at a time (no second register array):
+//   P̂ = (X[k] + conj(X[-k]))/2,  i Q̂ = (X[k] - conj(X[-k]))/2.
+// H(k) returns the kernel at bin k.  All threads of the block call it.
+template <typename R, int LOGN, int LOGE, class HF>
+__device__ __forceinline__ void split_pair_apply(cx<R> (&v)[1 << LOGE], void* __restrict__ smv,
+                                                 HF&& H) {
+    using S = FftShape<LOGN, LOGE>;
+    constexpr int E = S::E, T = S::T, N = S::N;
+    const int t = threadIdx.x;
+    if constexpr (!SmemPlan<R, LOGN>::SPLIT) {
+        cx<R>* sm = (cx<R>*)smv;
+#pragma unroll
+        for (int s = 0; s < E; s++) sm[pad(t + T * s)] = v[s];
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = t + T * s;
+            const cx<R> zm = conjc(sm[pad((N - b) & (N - 1))]);
+            const cx<R> h = H(b);
+            const cx<R> a = scale(v[s] + zm, R(0.5));
+            const cx<R> c = scale(v[s] - zm, R(0.5));
+            v[s] = cmul(a, h) + cmulc(c, h);
+        }
+        __syncthreads();
+    } else {
+        // real and imaginary parts in two rounds through a half-size buffer
+        R* sm = (R*)smv;
+        R xr[E];
+#pragma unroll
+        for (int s = 0; s < E; s++) sm[pad(t + T * s)] = v[s].re;
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) xr[s] = sm[pad((N - (t + T * s)) & (N - 1))];
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) sm[pad(t + T * s)] = v[s].im;
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int b = t + T * s;
+            const cx<R> zm = mk(xr[s], -sm[pad((N - b) & (N - 1))]);
+            const cx<R> h = H(b);
+            const cx<R> a = scale(v[s] + zm, R(0.5));
+            const cx<R> c = scale(v[s] - zm, R(0.5));
+            v[s] = cmul(a, h) + cmulc(c, h);
+        }
+        __syncthreads();
+    }
+}
+
 // Block-wide unnormalised forward transform (exponent sign -1) of the N
 // values held in v; all threads of the block call it.  The passes between
 // the first and the last run as a runtime loop over one code body, so a

@@ -241,17 +241,10 @@ struct SmSolver {
                     v[s] = mk(I, Y);
                 }
             } else if (op == 11) {
-                // split the two real spectra with X[k] and conj(X[-k])
-                C xm[E];
-                gather_negated<R, LOGN, LOGE>(v, xm, sm);
-#pragma unroll
-                for (int s = 0; s < E; s++) {
-                    const C zm = conjc(xm[s]);
-                    const C H = Heff[bin(s)];
-                    const C a = scale(v[s] + zm, R(0.5));   // spectrum of I
-                    const C c = scale(v[s] - zm, R(0.5));   // i * spectrum of Y
-                    v[s] = cmul(a, H) + cmulc(c, H);
-                }
+                // split the two real spectra (I and Y) with X[k] and conj(X[-k]);
+                // Heff Î + i conj(Heff) Ŷ
+                const C* __restrict__ Hp = Heff;
+                split_pair_apply<R, LOGN, LOGE>(v, sm, [Hp](int b) { return Hp[b]; });
                 inv = true;
             } else {  // op == 12
 #pragma unroll
