@@ -143,6 +143,7 @@ struct fl_problem {
     void* d_ss[2] = {nullptr, nullptr};
     void* d_tw[2] = {nullptr, nullptr};
     void* d_G[2] = {nullptr, nullptr};     // multimode contraction matrix [0] float, [1] double
+    double* d_Ga = nullptr;                // its adjoint layout
     // workspace of the last forward (kept for fl_adjoint)
     struct Work* last = nullptr;
     struct MmWork* mlast = nullptr;        // same for multimode problems
@@ -510,6 +511,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
             d.tw[q] = pr->d_tw[q];
             d.G[q] = pr->d_G[q];
         }
+        d.Ga = pr->d_Ga;
         d.M = pr->m;
         d.nparts = nparts;
         d.NP = w->np;
@@ -663,28 +665,33 @@ __global__ void mm_gather_J_kernel(const MmState* __restrict__ st, int n, double
     if (i < n) J[i] = st[i].J;
 }
 
-// G[(i*M + j)*NP + q] = γ[i,j,k,l] + γ[i,j,l,k] (k < l), γ[i,j,k,k] (k = l),
-// q enumerating k <= l row by row; γ in the reference's column-major order
+// G[(i*M + j)*GP + q] = γ[i,j,k,l] + γ[i,j,l,k] (k < l), γ[i,j,k,k] (k = l),
+// q enumerating k <= l row by row (GP: the pair count padded to 4 with zeros);
+// the adjoint's copy Ga[(j*NP + q)*MP + i] (MP: M padded to 2); γ in the
+// reference's column-major order
 int mm_upload_G(fl_problem* pr, const double* gamma) {
     fl_ctx* ctx = pr->ctx;
-    const int M = pr->m, NP = M * (M + 1) / 2;
+    const int M = pr->m, NP = M * (M + 1) / 2, GP = mm_gp(M), MP = mm_mp(M);
     auto g = [&](int i, int j, int k, int l) { return gamma[i + M * (j + M * (k + M * l))]; };
-    std::vector<double> G((size_t)M * M * NP);
-    std::vector<float> Gf(G.size());
+    std::vector<double> G((size_t)M * M * GP, 0.0), Ga((size_t)M * NP * MP, 0.0);
+    std::vector<float> Gf(G.size(), 0.f);
     for (int i = 0; i < M; i++)
         for (int j = 0; j < M; j++) {
             int q = 0;
             for (int k = 0; k < M; k++)
                 for (int l = k; l < M; l++, q++) {
                     const double v = k == l ? g(i, j, k, k) : g(i, j, k, l) + g(i, j, l, k);
-                    G[((size_t)i * M + j) * NP + q] = v;
-                    Gf[((size_t)i * M + j) * NP + q] = (float)v;
+                    G[((size_t)i * M + j) * GP + q] = v;
+                    Gf[((size_t)i * M + j) * GP + q] = (float)v;
+                    Ga[((size_t)j * NP + q) * MP + i] = v;
                 }
         }
     CU(cudaMalloc(&pr->d_G[0], sizeof(float) * Gf.size()));
     CU(cudaMalloc(&pr->d_G[1], sizeof(double) * G.size()));
+    CU(cudaMalloc(&pr->d_Ga, sizeof(double) * Ga.size()));
     CU(cudaMemcpy(pr->d_G[0], Gf.data(), sizeof(float) * Gf.size(), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(pr->d_G[1], G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(pr->d_Ga, Ga.data(), sizeof(double) * Ga.size(), cudaMemcpyHostToDevice));
     return FL_OK;
 }
 
@@ -993,6 +1000,7 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
             d.ss[q] = pr->d_ss[q];
             d.G[q] = pr->d_G[q];
         }
+        d.Ga = pr->d_Ga;
         d.one_m_fR = pr->one_m_fR;
         d.L = r->L;
         d.reltol = pr->reltol;
@@ -1373,6 +1381,7 @@ int fl_problem_destroy(fl_problem* pr) {
     delete pr->mlast;
     cudaFree(pr->d_G[0]);
     cudaFree(pr->d_G[1]);
+    cudaFree(pr->d_Ga);
     cudaFree(pr->d_Dturns);
     for (int q = 0; q < 2; q++) {
         cudaFree(pr->d_Heff[q]);

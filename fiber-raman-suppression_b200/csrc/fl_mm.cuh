@@ -412,6 +412,30 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     else dst = static_cast<C*>(mm_kp(d.kf, st.kperm, st.stage));
 #pragma unroll
     for (int s = 0; s < E; s++) dst[off + tid + TT * s] = v[s];
+    if (st.stage == 6 && ph == PH_REC) {
+        // dense interpolant of the replayed step, this mode's part:
+        // c0 = ũ_n, c_p = Σ_i r_ip k_i (Tsit5's free 4th-order interpolant)
+        const size_t NM = (size_t)N * d.M, base = (size_t)st.rec_pos * 5 * NM;
+        C* sg = static_cast<C*>(d.seg);
+        const double* un = d.u[st.cur];
+#pragma unroll 1
+        for (int s = 0; s < E; s++) {
+            const size_t b = off + tid + TT * s;
+            sg[base + b] = down<R>(ld2(un, b));
+            double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int i = 0; i < 7; i++) {
+                const C ki = i == 6 ? v[s] : static_cast<const C*>(mm_kp(d.kf, st.kperm, i))[b];
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    cr[q] += kT5r[i][q] * (double)ki.re;
+                    ci[q] += kT5r[i][q] * (double)ki.im;
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) sg[base + (q + 1) * NM + b] = mk((R)cr[q], (R)ci[q]);
+        }
+    }
     if (st.stage == 6 && (ph == PH_FWD || ph == PH_ADJ)) {
         const double dt = st.cdt, bt7 = kT5bt[6];
         double acc = 0.0;
@@ -434,34 +458,68 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
 // ---------------------------------------------------------------------------
 constexpr int kMmTB = 128;  // threads per block of the contraction kernels
 
+// Row lengths of the contraction tables: the pair axis of G padded to a
+// multiple of 4 (zeros) so rows load as float4 / double2 vectors, and the
+// mode axis of the adjoint table padded to even.
+template <int M>
+struct MmPairs {
+    static constexpr int NP = M * (M + 1) / 2;
+    static constexpr int GP = (NP + 3) & ~3;
+    static constexpr int MP = (M + 1) & ~1;
+};
+
+// acc[0..3] += row[q..q+3] * x[q..q+3] for q in [0, GP)
+template <int GP>
+__device__ __forceinline__ float dot_row(const float* __restrict__ row, const float (&x)[GP]) {
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+    for (int q = 0; q < GP; q += 4) {
+        const float4 g = __ldg(reinterpret_cast<const float4*>(row + q));
+        a0 += g.x * x[q];
+        a1 += g.y * x[q + 1];
+        a2 += g.z * x[q + 2];
+        a3 += g.w * x[q + 3];
+    }
+    return (a0 + a1) + (a2 + a3);
+}
+template <int GP>
+__device__ __forceinline__ double dot_row(const double* __restrict__ row, const double (&x)[GP]) {
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+    for (int q = 0; q < GP; q += 4) {
+        const double2 g0 = __ldg(reinterpret_cast<const double2*>(row + q));
+        const double2 g1 = __ldg(reinterpret_cast<const double2*>(row + q + 2));
+        a0 += g0.x * x[q];
+        a1 += g0.y * x[q + 1];
+        a2 += g1.x * x[q + 2];
+        a3 += g1.y * x[q + 3];
+    }
+    return (a0 + a1) + (a2 + a3);
+}
+
 // forward: η_i = Σ_j (Σ_q G[i,j,q] S_q) u_j, in precision R
 template <typename R, int M>
 __device__ __forceinline__ void mm_contract_fwd(const MmDesc& d, int t) {
-    constexpr int NP = M * (M + 1) / 2;
+    using PS = MmPairs<M>;
+    constexpr int NP = PS::NP, GP = PS::GP;
     const int N = d.N;
     const cx<R>* ut = static_cast<const cx<R>*>(d.ut);
     const R* sq = static_cast<const R*>(d.sq);
     const R* G = static_cast<const R*>(d.G[sizeof(R) == 8]);
     cx<R>* eta = static_cast<cx<R>*>(d.eta);
     cx<R> u[M];
-    R Sv[NP];
+    R Sv[GP];
 #pragma unroll
     for (int j = 0; j < M; j++) u[j] = ut[(size_t)j * N + t];
 #pragma unroll
-    for (int q = 0; q < NP; q++) Sv[q] = sq[(size_t)q * N + t];
+    for (int q = 0; q < GP; q++) Sv[q] = q < NP ? sq[(size_t)q * N + t] : R(0);
 #pragma unroll 1
     for (int i = 0; i < M; i++) {
-        const R* Gi = G + (size_t)i * M * NP;
+        const R* Gi = G + (size_t)i * M * GP;
         R er = R(0), ei = R(0);
 #pragma unroll
         for (int j = 0; j < M; j++) {
-            R a0 = R(0), a1 = R(0);
-#pragma unroll
-            for (int q = 0; q < NP; q += 2) {
-                a0 += __ldg(Gi + j * NP + q) * Sv[q];
-                if (q + 1 < NP) a1 += __ldg(Gi + j * NP + q + 1) * Sv[q + 1];
-            }
-            const R dij = a0 + a1;
+            const R dij = dot_row<GP>(Gi + j * GP, Sv);
             er += dij * u[j].re;
             ei += dij * u[j].im;
         }
@@ -473,13 +531,14 @@ __device__ __forceinline__ void mm_contract_fwd(const MmDesc& d, int t) {
 // Yh_q = (Im(λ_k u_l*) + Im(λ_l u_k*))/2 (k < l), Im(λ_k u_k*) (k = l)
 template <int M>
 __device__ __forceinline__ void mm_imx(const MmDesc& d, int t) {
-    constexpr int NP = M * (M + 1) / 2;
+    using PS = MmPairs<M>;
+    constexpr int NP = PS::NP, GP = PS::GP;
     const int N = d.N;
     const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
     const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
     const double* G = static_cast<const double*>(d.G[1]);
     double* cq = static_cast<double*>(d.cq);
-    double Y[NP];
+    double Y[GP];
     {
         cx<double> la[M], u[M];
 #pragma unroll
@@ -497,42 +556,40 @@ __device__ __forceinline__ void mm_imx(const MmDesc& d, int t) {
                 Y[q++] = k == l ? a : 0.5 * (a + b);
             }
         }
+#pragma unroll
+        for (int r = NP; r < GP; r++) Y[r] = 0.0;
     }
 #pragma unroll 1
     for (int p = 0; p < NP; p++) {
         int i, j;
         pair_kl(p, M, i, j);
-        const double* Gr = G + ((size_t)i * M + j) * NP;
-        double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-        for (int q = 0; q < NP; q += 2) {
-            a0 += __ldg(Gr + q) * Y[q];
-            if (q + 1 < NP) a1 += __ldg(Gr + q + 1) * Y[q + 1];
-        }
-        cq[(size_t)p * N + t] = a0 + a1;
+        cq[(size_t)p * N + t] = dot_row<GP>(G + ((size_t)i * M + j) * GP, Y);
     }
 }
 
 // adjoint, second pass (thread per (t, j)):
 //   η_j = Σ_q S'_q g_q - (1-fR) Σ_q (u_k u_l) conj(g_q) + 2i Σ_i C_ij u_i,
-//   g_q = Σ_i λ_i G[i,j,q]
+//   g_q = Σ_i λ_i G[i,j,q], read from the table Ga[(j*NP + q)*MP + i]
 template <int M>
 __device__ __forceinline__ void mm_contract_adj(const MmDesc& d, int t, int j) {
-    constexpr int NP = M * (M + 1) / 2;
+    using PS = MmPairs<M>;
+    constexpr int NP = PS::NP, MP = PS::MP;
     const int N = d.N;
     const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
     const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
     const double* sq = static_cast<const double*>(d.sq);
     const double* cq = static_cast<const double*>(d.cq);
-    const double* G = static_cast<const double*>(d.G[1]);
+    const double* Ga = d.Ga + (size_t)j * NP * MP;
     cx<double>* eta = static_cast<cx<double>*>(d.eta);
     const double ofr = d.one_m_fR;
-    cx<double> la[M], u[M];
+    cx<double> la[MP], u[M];
 #pragma unroll
     for (int i = 0; i < M; i++) {
         la[i] = lt[(size_t)i * N + t];
         u[i] = ut[(size_t)i * N + t];
     }
+#pragma unroll
+    for (int i = M; i < MP; i++) la[i] = mk(0.0, 0.0);
     double er = 0.0, ei = 0.0;
     int q = 0;
 #pragma unroll
@@ -541,10 +598,10 @@ __device__ __forceinline__ void mm_contract_adj(const MmDesc& d, int t, int j) {
         for (int l = k; l < M; l++) {
             double gr = 0.0, gi = 0.0;
 #pragma unroll
-            for (int i = 0; i < M; i++) {
-                const double g = __ldg(G + ((size_t)i * M + j) * NP + q);
-                gr += g * la[i].re;
-                gi += g * la[i].im;
+            for (int i = 0; i < MP; i += 2) {
+                const double2 g = __ldg(reinterpret_cast<const double2*>(Ga + (size_t)q * MP + i));
+                gr += g.x * la[i].re + g.y * la[i + 1].re;
+                gi += g.x * la[i].im + g.y * la[i + 1].im;
             }
             const double s = sq[(size_t)q * N + t];
             const cx<double> w = cmul(u[k], u[l]);
@@ -722,22 +779,7 @@ struct MmCtl {
             const double* u = d.u[st.cur];
             const bool f64 = d.fp64 != 0;
             if (ph == PH_REC) {
-                // interpolant of this step: c0 = ũ_n, c_p = Σ_i r_ip k_i
-                const size_t base = (size_t)st.rec_pos * 5 * NM;
-                for (size_t i = threadIdx.x; i < NM; i += kMmCtl) {
-                    stcr(d.seg, base + i, ld2(u, i), f64);
-                    double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
-                    for (int s = 0; s < 7; s++) {
-                        const cx<double> ks = ldcr(mm_kp(d.kf, st.kperm, s), i, f64);
-#pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            cr[q] += kT5r[s][q] * ks.re;
-                            ci[q] += kT5r[s][q] * ks.im;
-                        }
-                    }
-#pragma unroll
-                    for (int q = 0; q < 4; q++) stcr(d.seg, base + (q + 1) * NM + i, mk(cr[q], ci[q]), f64);
-                }
+                // (the epilogue has stored this step's dense interpolant)
                 st.cur ^= 1;
                 st.kperm ^= 1;
                 st.rec_pos++;

@@ -93,6 +93,12 @@ struct SlotState {
 };
 
 // ---------------------------------------------------------------------------
+// Padded row lengths of the multimode contraction tables: the pair axis
+// (M(M+1)/2) padded to 4 and the mode axis padded to 2 (vector loads).
+__host__ __device__ constexpr int mm_gp(int M) { return (M * (M + 1) / 2 + 3) & ~3; }
+__host__ __device__ constexpr int mm_mp(int M) { return (M + 1) & ~1; }
+
+// ---------------------------------------------------------------------------
 // Multimode (M > 1) slots.  One right-hand-side evaluation runs as a chain of
 // kernels over every active slot (mode transforms, pair convolutions, per-time
 // contractions), and a control kernel advances each slot's integrator between
@@ -104,7 +110,8 @@ struct MmDesc {
     const void* Heff[2];    // cx: hR * (-1)^k
     const void* ss[2];      // real: fftshift(ωs/ω0)
     const void* tw[2];      // cx: exp(-2 pi i k / N)
-    const void* G[2];       // M*M*NP: G[(i*M + j)*NP + q] (pair q = (k <= l))
+    const void* G[2];       // M*M*GP: G[(i*M + j)*GP + q] (pair q = (k <= l); GP = NP padded to 4)
+    const double* Ga;       // NP*M*MP: the same values as Ga[(j*NP + q)*MP + i] (MP = M padded to 2)
     int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
     int nparts;             // error partial sums per evaluation (M x CTAs per transform)
     double one_m_fR;
