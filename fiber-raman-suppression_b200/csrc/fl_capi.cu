@@ -840,6 +840,7 @@ double now_ms() {
 
 struct SrvRequest {
     long id = 0;
+    int weight = 1;                    // CTAs per transform of its slot
     fl_problem* prob = nullptr;
     int kind = FL_REQ_FORWARD, log_cost = 0;
     double L = 0;
@@ -882,7 +883,6 @@ struct SrvBucket {
     bool mm = false;
     fl_problem* tables = nullptr;      // server-owned twiddles (and defaults) for free slots
     std::vector<SrvChunk*> chunks;
-    std::deque<SrvRequest*> pending;
     ~SrvBucket() {
         for (auto* c : chunks) delete c;
         if (tables) fl_problem_destroy(tables);
@@ -896,7 +896,10 @@ struct fl_server {
     std::mutex mu;
     std::condition_variable cv;
     std::map<long, SrvRequest*> reqs;
-    std::deque<SrvRequest*> incoming;
+    std::deque<SrvRequest*> incoming;      // submitted, not yet seen by the progress thread
+    std::deque<SrvRequest*> waiting;       // arrival order, not yet in a slot (progress thread)
+    std::atomic<long> n_waiting{0};
+    long active_w = 0;                     // CTAs per transform of the requests in slots
     std::vector<SrvBucket*> buckets;
     size_t hbm_used = 0;
     long next_id = 1, submitted = 0, completed = 0, launches = 0;
@@ -920,9 +923,10 @@ size_t srv_slot_bytes(const fl_server* sv, const fl_problem* pr) {
            16 * nm * 4 + 8 * nm + 2 * (size_t)pr->nt;
 }
 
-int srv_chunk_slots(const SrvBucket* b) {
-    if (!b->mm) return 148;
-    return std::max(1, 148 / (b->m * mm_cluster_ctas(ilog2i(b->nt))));
+int srv_chunk_slots(const fl_server* sv, const SrvBucket* b) {
+    const int cap = std::max(1, std::min(sv->opts.max_active_ctas, std::max(1, sv->ctx->sm_count)));
+    if (!b->mm) return cap;
+    return std::max(1, cap / (b->m * mm_cluster_ctas(ilog2i(b->nt))));
 }
 
 // a bucket's own table set: a problem with this shape's grid (zero tables),
@@ -940,7 +944,7 @@ int srv_new_chunk(fl_server* sv, SrvBucket* b) {
     fl_ctx* ctx = sv->ctx;
     auto c = std::make_unique<SrvChunk>();
     c->mm = b->mm;
-    c->B = srv_chunk_slots(b);
+    c->B = srv_chunk_slots(sv, b);
     const size_t need = srv_slot_bytes(sv, b->tables) * c->B;
     if (sv->opts.hbm_budget_bytes && sv->hbm_used + need > sv->opts.hbm_budget_bytes) {
         // a smaller chunk if at least one slot fits
@@ -1130,65 +1134,91 @@ SrvBucket* srv_bucket_for(fl_server* sv, const fl_problem* pr) {
     return nullptr;
 }
 
-// One pass over every bucket; returns whether anything happened.
+SrvBucket* srv_bucket_get(fl_server* sv, const fl_problem* pr, int& rc) {
+    rc = FL_OK;
+    SrvBucket* b = srv_bucket_for(sv, pr);
+    if (b) return b;
+    b = new SrvBucket();
+    b->nt = pr->nt;
+    b->m = pr->m;
+    b->precision = pr->precision;
+    b->mm = pr->use_mm;
+    sv->buckets.push_back(b);
+    rc = srv_bucket_tables(sv, b);
+    return b;
+}
+
+// One pass: retire finished launches, admit waiting requests in arrival
+// order while the requests in flight fit the SMs (and the HBM budget allows
+// their slots), launch every chunk with work.  Returns whether anything
+// happened.
 int srv_progress(fl_server* sv, bool& did) {
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         while (!sv->incoming.empty()) {
-            SrvRequest* r = sv->incoming.front();
+            sv->waiting.push_back(sv->incoming.front());
             sv->incoming.pop_front();
-            SrvBucket* b = srv_bucket_for(sv, r->prob);
-            if (!b) {
-                b = new SrvBucket();
-                b->nt = r->prob->nt;
-                b->m = r->prob->m;
-                b->precision = r->prob->precision;
-                b->mm = r->prob->use_mm;
-                sv->buckets.push_back(b);
-                int rc = srv_bucket_tables(sv, b);
-                if (rc) return rc;
-            }
-            b->pending.push_back(r);
             did = true;
         }
     }
     std::vector<std::pair<SrvRequest*, int>> done;
-    for (auto* b : sv->buckets) {
+    for (auto* b : sv->buckets)
         for (auto* c : b->chunks) {
-            if (c->inflight) {
-                const cudaError_t q = cudaEventQuery(c->ev);
-                if (q == cudaErrorNotReady) continue;
-                if (q != cudaSuccess) {
-                    fl_ctx* ctx = sv->ctx;
-                    CU(q);
-                }
-                c->inflight = false;
-                int rc = srv_retire(sv, b, c, done);
-                if (rc) return rc;
-                did = true;
+            if (!c->inflight) continue;
+            const cudaError_t q = cudaEventQuery(c->ev);
+            if (q == cudaErrorNotReady) continue;
+            if (q != cudaSuccess) {
+                fl_ctx* ctx = sv->ctx;
+                CU(q);
             }
-            for (int i = 0; i < c->B && !b->pending.empty(); i++)
+            c->inflight = false;
+            const size_t before = done.size();
+            int rc = srv_retire(sv, b, c, done);
+            if (rc) return rc;
+            for (size_t k = before; k < done.size(); k++) sv->active_w -= done[k].first->weight;
+            did = true;
+        }
+    const long cap = sv->opts.max_active_ctas;
+    while (!sv->waiting.empty()) {
+        SrvRequest* r = sv->waiting.front();
+        if (sv->active_w > 0 && sv->active_w + r->weight > cap) break;
+        int rc;
+        SrvBucket* b = srv_bucket_get(sv, r->prob, rc);
+        if (rc) return rc;
+        SrvChunk* fc = nullptr;
+        int fi = -1;
+        for (auto* c : b->chunks) {
+            for (int i = 0; i < c->B && fi < 0; i++)
                 if (!c->slot[i]) {
-                    int rc = srv_admit(sv, b, c, i, b->pending.front());
-                    if (rc) return rc;
-                    b->pending.pop_front();
-                    did = true;
+                    fc = c;
+                    fi = i;
                 }
+            if (fc) break;
+        }
+        if (!fc) {
+            rc = srv_new_chunk(sv, b);
+            if (rc == FL_OOM_ADMISSION) break;  // wait for slots to free up
+            if (rc) return rc;
+            fc = b->chunks.back();
+            fi = 0;
+        }
+        rc = srv_admit(sv, b, fc, fi, r);
+        if (rc) return rc;
+        sv->active_w += r->weight;
+        sv->waiting.pop_front();
+        did = true;
+    }
+    sv->n_waiting.store((long)sv->waiting.size());
+    for (auto* b : sv->buckets)
+        for (auto* c : b->chunks) {
+            if (c->inflight) continue;
             bool any = false;
             for (auto* r : c->slot) any |= r != nullptr;
-            if (any) {
-                int rc = srv_launch(sv, b, c);
-                if (rc) return rc;
-                did = true;
-            }
+            if (!any) continue;
+            int rc = srv_launch(sv, b, c);
+            if (rc) return rc;
+            did = true;
         }
-        // grow while requests wait and the budget allows
-        if (!b->pending.empty()) {
-            const int rc = srv_new_chunk(sv, b);
-            if (rc == FL_OK) did = true;
-            else if (rc != FL_OOM_ADMISSION) return rc;
-        }
-    }
     if (!done.empty()) {
         const double t = now_ms();
         std::lock_guard<std::mutex> lk(sv->mu);
@@ -1675,6 +1705,10 @@ int fl_server_create(fl_ctx* ctx, const fl_server_opts* opts, fl_server** out) {
         if (opts->checkpoints > 0) sv->opts.checkpoints = opts->checkpoints;
         if (opts->segment_steps > 0) sv->opts.segment_steps = opts->segment_steps;
     }
+    // default: no cap beyond slots and memory (a cap at the SM count trades
+    // median latency for nothing on a heavy-tailed stream)
+    sv->opts.max_active_ctas =
+        opts && opts->max_active_ctas > 0 ? opts->max_active_ctas : 1 << 30;
     if (!pow2(sv->opts.checkpoints) || sv->opts.checkpoints < 2)
         return set_err(ctx, FL_EINVAL, "server checkpoints must be a power of two >= 2");
     sv->wopts = ctx->opts;
@@ -1731,6 +1765,7 @@ int fl_server_submit(fl_server* sv, const fl_request* q, long* id) {
     if (!std::isfinite(L)) return set_err(ctx, FL_EINVAL, "L must be positive and finite");
     auto r = std::make_unique<SrvRequest>();
     r->prob = pr;
+    r->weight = pr->use_mm ? pr->m * mm_cluster_ctas(logn) : 1;
     r->kind = q->kind;
     r->log_cost = q->log_cost;
     r->L = L;
@@ -1809,7 +1844,7 @@ int fl_server_info_get(fl_server* sv, fl_server_info* info) {
     std::lock_guard<std::mutex> lk(sv->mu);
     info->submitted = sv->submitted;
     info->completed = sv->completed;
-    info->queued = (long)sv->incoming.size();
+    info->queued = (long)sv->incoming.size() + sv->n_waiting.load();
     info->in_flight = sv->submitted - sv->completed;
     int slots = 0, chunks = 0;
     for (auto* b : sv->buckets) {

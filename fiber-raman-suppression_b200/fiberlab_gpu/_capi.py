@@ -47,7 +47,8 @@ class FlStats(C.Structure):
 
 class FlServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("evals_per_launch", C.c_int),
-                ("checkpoints", C.c_int), ("segment_steps", C.c_int)]
+                ("checkpoints", C.c_int), ("segment_steps", C.c_int),
+                ("max_active_ctas", C.c_int)]
 
 
 class FlRequest(C.Structure):

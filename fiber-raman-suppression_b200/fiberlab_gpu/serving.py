@@ -44,9 +44,10 @@ class Request:
 
 class Server:
     def __init__(self, ctx, hbm_budget_bytes: int = 0, evals_per_launch: int = 0,
-                 checkpoints: int = 0, segment_steps: int = 0):
+                 checkpoints: int = 0, segment_steps: int = 0, max_active_ctas: int = 0):
         self.ctx = ctx
-        opts = FlServerOpts(hbm_budget_bytes, evals_per_launch, checkpoints, segment_steps)
+        opts = FlServerOpts(hbm_budget_bytes, evals_per_launch, checkpoints, segment_steps,
+                            max_active_ctas)
         h = C.c_void_p()
         ctx.check(load().fl_server_create(ctx.h, C.byref(opts), C.byref(h)))
         self.h = h

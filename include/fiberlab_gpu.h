@@ -203,7 +203,8 @@ int fl_forward_noalloc(int device, int nt, const double *d_D, double gamma, cons
  * precision) into buckets of slots; each chunk of slots is advanced by a
  * bounded number of right-hand-side evaluations per launch on its own
  * stream, and between launches finished slots are retired (results copied
- * to the caller's buffers) and queued requests admitted into free slots.
+ * to the caller's buffers) and queued requests admitted into free slots, in
+ * arrival order (within an optional cap on requests in flight).
  * New chunks are allocated while the HBM budget allows.  All server calls
  * are thread-safe.  Problems referenced by requests must outlive them.
  * ------------------------------------------------------------------------ */
@@ -217,6 +218,9 @@ typedef struct {
     int segment_steps;        /* recompute segment length (default 128); a band-gradient
                                  request holds up to checkpoints x segment_steps accepted
                                  forward steps (FL_ECAPACITY beyond) */
+    int max_active_ctas;      /* cap on requests in flight, counted in CTAs per transform (one
+                                 per single-CTA slot, M x cluster CTAs per multimode slot);
+                                 0: no cap beyond slots and the HBM budget */
 } fl_server_opts;
 
 typedef struct {
