@@ -591,6 +591,7 @@ MmRound mm_round_args(fl_problem* pr, MmWork* w, int nactive) {
     a.N = pr->nt;
     a.fp64 = pr->precision == FL_PRECISION_FP64;
     a.control = 1;
+    a.tensor_cores = 1;
     a.ndone = nullptr;
     a.stream = pr->ctx->stream;
     return a;
@@ -1110,6 +1111,7 @@ int srv_launch(fl_server* sv, SrvBucket* b, SrvChunk* c) {
         a.N = b->nt;
         a.fp64 = b->precision == FL_PRECISION_FP64;
         a.control = 1;
+        a.tensor_cores = 1;
         a.ndone = nullptr;
         a.stream = c->stream;
         MmRoundFn round = mm_round_launcher(logn);

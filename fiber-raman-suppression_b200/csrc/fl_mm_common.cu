@@ -3,6 +3,7 @@
 // the table of evaluation rounds per grid size.
 #include "fl_mm.cuh"
 #include "fl_mm_launch.h"
+#include "fl_tc.cuh"
 
 namespace fl {
 
@@ -43,10 +44,41 @@ __global__ void __launch_bounds__(kMmCtl)
 }
 
 
+// The FP32 forward contraction on the tensor cores (M >= 6, Nt a multiple
+// of 128): one 128-point tile per CTA.
+template <int M>
+__global__ void __launch_bounds__(kTcRows)
+    mm_contract_tc_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
+                          const int* __restrict__ active) {
+    extern __shared__ __align__(16) unsigned char tc_smem[];
+    const int slot = active[blockIdx.y];
+    const MmDesc& d = descs[slot];
+    if (d.M != M) return;
+    const MmState st = states[slot];
+    if (!mm_takes<float>(d, st) || mm_adjoint_phase(st.phase)) return;
+    mm_contract_fwd_tc<M>(d, blockIdx.x * kTcRows, tc_smem);
+}
+
 namespace {
+
+template <int M>
+cudaError_t contract_tc(const MmRound& a) {
+    const size_t smem = TcShape<M>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(mm_contract_tc_kernel<M>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(a.N / kTcRows, a.nactive);
+    mm_contract_tc_kernel<M><<<grid, kTcRows, smem, a.stream>>>(
+        static_cast<const MmDesc*>(a.desc), a.state, a.active);
+    return cudaGetLastError();
+}
 
 template <typename R, int M>
 cudaError_t contract_m(const MmRound& a, int which) {
+    // FP32 forward with M >= 6 modes: tensor cores (3xTF32)
+    if constexpr (sizeof(R) == 4 && M >= 6) {
+        if (which == 0 && a.tensor_cores && a.N % kTcRows == 0) return contract_tc<M>(a);
+    }
     const int n = which == 2 ? a.N * M : a.N;
     const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);
     mm_contract_kernel<R, M><<<grid, kMmTB, 0, a.stream>>>(static_cast<const MmDesc*>(a.desc),

@@ -16,6 +16,7 @@ struct MmRound {
     int M, NP, N;          // modes, pairs, points (same for every slot of the batch)
     int fp64;              // forward precision of the batch
     int control;           // run the control kernel after the evaluation
+    int tensor_cores;      // FP32 forward contraction on tcgen05 when M >= 6
     int* ndone;            // control: count of finished slots (nullable)
     cudaStream_t stream;
 };
