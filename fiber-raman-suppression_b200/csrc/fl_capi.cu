@@ -144,6 +144,7 @@ struct fl_problem {
     void* d_tw[2] = {nullptr, nullptr};
     void* d_G[2] = {nullptr, nullptr};     // multimode contraction matrix [0] float, [1] double
     double* d_Ga = nullptr;                // its adjoint layout
+    float* d_Gtc = nullptr;                // its tensor-core operand image (M >= 6)
     // workspace of the last forward (kept for fl_adjoint)
     struct Work* last = nullptr;
     struct MmWork* mlast = nullptr;        // same for multimode problems
@@ -512,6 +513,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
             d.G[q] = pr->d_G[q];
         }
         d.Ga = pr->d_Ga;
+        d.Gtc = pr->d_Gtc;
         d.M = pr->m;
         d.nparts = nparts;
         d.NP = w->np;
@@ -693,6 +695,32 @@ int mm_upload_G(fl_problem* pr, const double* gamma) {
     CU(cudaMemcpy(pr->d_G[0], Gf.data(), sizeof(float) * Gf.size(), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(pr->d_G[1], G.data(), sizeof(double) * G.size(), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(pr->d_Ga, Ga.data(), sizeof(double) * Ga.size(), cudaMemcpyHostToDevice));
+    if (M >= 6) {
+        // B operand of the tensor-core contraction: rows ij (padded to a multiple
+        // of 16), pairs (padded to 8), split into TF32 hi + lo (round to
+        // nearest: 10-bit mantissa), laid out as the kernel's shared memory
+        const int KP = (NP + 7) & ~7, NN = (M * M + 15) & ~15;
+        const size_t bbytes = (size_t)NN * KP * 4;
+        std::vector<unsigned char> img(2 * bbytes, 0);
+        auto tf32 = [](float x) {
+            uint32_t u;
+            memcpy(&u, &x, 4);
+            if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+            float r;
+            memcpy(&r, &u, 4);
+            return r;
+        };
+        for (int r = 0; r < M * M; r++)
+            for (int k = 0; k < NP; k++) {
+                const float g = Gf[(size_t)r * GP + k];
+                const float hi = tf32(g), lo = tf32(g - hi);
+                const uint32_t off = (uint32_t)((r >> 3) * (KP * 32) + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
+                memcpy(&img[off], &hi, 4);
+                memcpy(&img[bbytes + off], &lo, 4);
+            }
+        CU(cudaMalloc(&pr->d_Gtc, img.size()));
+        CU(cudaMemcpy(pr->d_Gtc, img.data(), img.size(), cudaMemcpyHostToDevice));
+    }
     return FL_OK;
 }
 
@@ -1006,6 +1034,7 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
             d.G[q] = pr->d_G[q];
         }
         d.Ga = pr->d_Ga;
+        d.Gtc = pr->d_Gtc;
         d.one_m_fR = pr->one_m_fR;
         d.L = r->L;
         d.reltol = pr->reltol;
@@ -1414,6 +1443,7 @@ int fl_problem_destroy(fl_problem* pr) {
     cudaFree(pr->d_G[0]);
     cudaFree(pr->d_G[1]);
     cudaFree(pr->d_Ga);
+    cudaFree(pr->d_Gtc);
     cudaFree(pr->d_Dturns);
     for (int q = 0; q < 2; q++) {
         cudaFree(pr->d_Heff[q]);

@@ -1,6 +1,8 @@
 // fl_mm_common.cu -- grid-size-independent multimode kernels (per-time
 // contractions for each built mode count, the per-slot control kernel) and
 // the table of evaluation rounds per grid size.
+#include <algorithm>
+
 #include "fl_mm.cuh"
 #include "fl_mm_launch.h"
 #include "fl_tc.cuh"
@@ -45,7 +47,7 @@ __global__ void __launch_bounds__(kMmCtl)
 
 
 // The FP32 forward contraction on the tensor cores (M >= 6, Nt a multiple
-// of 128): one 128-point tile per CTA.
+// of 128): CTAs loop over a slot's 128-point tiles.
 template <int M>
 __global__ void __launch_bounds__(kTcRows)
     mm_contract_tc_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
@@ -56,7 +58,7 @@ __global__ void __launch_bounds__(kTcRows)
     if (d.M != M) return;
     const MmState st = states[slot];
     if (!mm_takes<float>(d, st) || mm_adjoint_phase(st.phase)) return;
-    mm_contract_fwd_tc<M>(d, blockIdx.x * kTcRows, tc_smem);
+    mm_contract_fwd_tc<M>(d, blockIdx.x, gridDim.x, tc_smem);
 }
 
 namespace {
@@ -67,6 +69,8 @@ cudaError_t contract_tc(const MmRound& a) {
     cudaError_t e = cudaFuncSetAttribute(mm_contract_tc_kernel<M>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    // one 128-point tile per CTA (many CTAs in flight hide each tile's
+    // load -> MMA -> drain chain better than a persistent loop)
     const dim3 grid(a.N / kTcRows, a.nactive);
     mm_contract_tc_kernel<M><<<grid, kTcRows, smem, a.stream>>>(
         static_cast<const MmDesc*>(a.desc), a.state, a.active);

@@ -50,6 +50,9 @@ struct TcShape {
 };
 
 // byte offset of element (row r, k) in a K-major no-swizzle tile
+__host__ __device__ constexpr uint32_t tc_off_rt(int r, int k, int KP) {
+    return (uint32_t)((r >> 3) * (KP * 32) + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
+}
 template <int KP>
 __device__ __forceinline__ uint32_t tc_off(int r, int k) {
     return (uint32_t)((r >> 3) * (KP * 32) + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
@@ -82,13 +85,17 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-// the forward contraction of one 128-point tile of one slot
+// The forward contraction of the 128-point tiles t0 = tile*128, tile =
+// first, first + step, ... < N/128 of one slot.  The B operand (the G table,
+// split hi/lo) and the tensor memory are set up once per CTA; each tile
+// refills A, issues its MMAs and waits on the barrier's next phase.
 template <int M>
-__device__ void mm_contract_fwd_tc(const MmDesc& d, int t0, unsigned char* smem) {
+__device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigned char* smem) {
     using TS = TcShape<M>;
     constexpr int NP = TS::NP, KP = TS::KP, GP = TS::GP, NN = TS::NN;
-    const int N = d.N;
+    const int N = d.N, ntiles = N / kTcRows;
     const int tid = threadIdx.x, warp = tid >> 5;
+    (void)GP;
     // 1024-byte aligned operand area
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
@@ -111,115 +118,138 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int t0, unsigned char* smem)
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
 
-    // ---- operands: B = G rows (ij) x pairs, A = S tile (t) x pairs, split hi/lo
-    const float* G = static_cast<const float*>(d.G[0]);
-    for (int e = tid; e < NN * KP; e += kTcRows) {
-        const int r = e / KP, k = e - r * KP;
-        const float g = (r < M * M && k < NP) ? __ldg(G + (size_t)r * GP + k) : 0.f;
-        const float hi = tf32_rn(g);
-        *reinterpret_cast<float*>(Bhi + tc_off<KP>(r, k)) = hi;
-        *reinterpret_cast<float*>(Blo + tc_off<KP>(r, k)) = tf32_rn(g - hi);
+    // ---- B = G rows (ij) x pairs, split hi/lo: a copy of the image prepared
+    // once per problem in exactly this shared-memory layout (B_hi then B_lo)
+    {
+        const int4* src = reinterpret_cast<const int4*>(d.Gtc);
+        int4* dst = reinterpret_cast<int4*>(Bhi);
+        for (int e = tid; e < 2 * TS::B_BYTES / 16; e += kTcRows) dst[e] = __ldg(src + e);
     }
+
     const float* sq = static_cast<const float*>(d.sq);
-    const int t = t0 + tid;
-#pragma unroll 4
-    for (int k = 0; k < KP; k++) {
-        const float s = k < NP ? sq[(size_t)k * N + t] : 0.f;
-        const float hi = tf32_rn(s);
-        *reinterpret_cast<float*>(Ahi + tc_off<KP>(tid, k)) = hi;
-        *reinterpret_cast<float*>(Alo + tc_off<KP>(tid, k)) = tf32_rn(s - hi);
-    }
-    // generic-proxy shared stores -> visible to the tensor core (async proxy)
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-
-    // ---- 3 x KP/8 MMAs from one thread, committed to the barrier
-    if (tid == 0) {
-        constexpr uint32_t idesc = tc_idesc(NN);
-        const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
-        const uint32_t b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
-#pragma unroll
-        for (int ks = 0; ks < KP / 8; ks++) {
-            const uint32_t koff = (uint32_t)ks * 256;
-            const uint64_t dah = tc_desc(a_hi + koff, 128, TS::SBO);
-            const uint64_t dal = tc_desc(a_lo + koff, 128, TS::SBO);
-            const uint64_t dbh = tc_desc(b_hi + koff, 128, TS::SBO);
-            const uint64_t dbl = tc_desc(b_lo + koff, 128, TS::SBO);
-            const uint32_t acc0 = ks > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         smem_u32(mbar))
-                     : "memory");
-    }
-
-    // ---- bounded wait for the MMAs (phase 0 of the barrier)
-    uint32_t done = 0;
-    for (long it = 0; it < (1L << 26) && !done; it++) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(smem_u32(mbar)), "r"(0u)
-            : "memory");
-    }
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    // ---- this thread's row of D: columns ij = i*M + j
-    float dv[NN];
-    if (done) {
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-        for (int c = 0; c < NN; c += 16) {
-            uint32_t r[16];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, "
-                "%10, %11, %12, %13, %14, %15}, [%16];\n"
-                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                  "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
-                  "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-                : "r"(taddr + (uint32_t)c));
-#pragma unroll
-            for (int q = 0; q < 16; q++) dv[c + q] = __uint_as_float(r[q]);
-        }
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    }
-
-    // ---- η_i = Σ_j δ_ij u_j
     const cx<float>* ut = static_cast<const cx<float>*>(d.ut);
     cx<float>* eta = static_cast<cx<float>*>(d.eta);
-    cx<float> u[M];
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int tile = first; tile < ntiles; tile += step) {
+        const int t = tile * kTcRows + tid;
+        if (!ok) {  // an earlier tile timed out: no more MMAs from this CTA
 #pragma unroll
-    for (int j = 0; j < M; j++) u[j] = ut[(size_t)j * N + t];
-#pragma unroll
-    for (int i = 0; i < M; i++) {
-        float er = 0.f, ei = 0.f;
-#pragma unroll
-        for (int j = 0; j < M; j++) {
-            er += dv[i * M + j] * u[j].re;
-            ei += dv[i * M + j] * u[j].im;
+            for (int i = 0; i < M; i++) eta[(size_t)i * N + t] = mk(__int_as_float(0x7fc00000), 0.f);
+            continue;
         }
-        eta[(size_t)i * N + t] = done ? mk(er, ei) : mk(__int_as_float(0x7fc00000), 0.f);
+        // ---- A = this tile's S, split hi/lo: four pairs per 16-byte store
+#pragma unroll 2
+        for (int k = 0; k < KP; k += 4) {
+            float4 hi, lo;
+            float* h = &hi.x;
+            float* l = &lo.x;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                const float s = k + c < NP ? sq[(size_t)(k + c) * N + t] : 0.f;
+                h[c] = tf32_rn(s);
+                l[c] = tf32_rn(s - h[c]);
+            }
+            *reinterpret_cast<float4*>(Ahi + tc_off<KP>(tid, k)) = hi;
+            *reinterpret_cast<float4*>(Alo + tc_off<KP>(tid, k)) = lo;
+        }
+        // generic-proxy shared stores -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tmem = *tmem_slot;
+
+        // ---- 3 x KP/8 MMAs from one thread, committed to the barrier
+        if (tid == 0) {
+            constexpr uint32_t idesc = tc_idesc(NN);
+            const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
+            const uint32_t b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
+#pragma unroll
+            for (int ks = 0; ks < KP / 8; ks++) {
+                const uint32_t koff = (uint32_t)ks * 256;
+                const uint64_t dah = tc_desc(a_hi + koff, 128, TS::SBO);
+                const uint64_t dal = tc_desc(a_lo + koff, 128, TS::SBO);
+                const uint64_t dbh = tc_desc(b_hi + koff, 128, TS::SBO);
+                const uint64_t dbl = tc_desc(b_lo + koff, 128, TS::SBO);
+                const uint32_t acc0 = ks > 0 ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(mbar))
+                : "memory");
+        }
+
+        // ---- bounded wait for this tile's MMAs (the barrier's current phase)
+        uint32_t done = 0;
+        for (long it = 0; it < (1L << 26) && !done; it++) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(done)
+                : "r"(smem_u32(mbar)), "r"(phase)
+                : "memory");
+        }
+        phase ^= 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        ok = ok && done;
+
+        // ---- this thread's row of D: columns ij = i*M + j
+        float dv[NN];
+        if (ok) {
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+            for (int c = 0; c < NN; c += 16) {
+                uint32_t r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, "
+                    "%9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                      "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                      "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                    : "r"(taddr + (uint32_t)c));
+#pragma unroll
+                for (int q = 0; q < 16; q++) dv[c + q] = __uint_as_float(r[q]);
+            }
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+        // the next tile's MMAs overwrite the accumulator and A: all reads done first
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+
+        // ---- η_i = Σ_j δ_ij u_j
+        cx<float> u[M];
+#pragma unroll
+        for (int j = 0; j < M; j++) u[j] = ut[(size_t)j * N + t];
+#pragma unroll
+        for (int i = 0; i < M; i++) {
+            float er = 0.f, ei = 0.f;
+#pragma unroll
+            for (int j = 0; j < M; j++) {
+                er += dv[i * M + j] * u[j].re;
+                ei += dv[i * M + j] * u[j].im;
+            }
+            eta[(size_t)i * N + t] = ok ? mk(er, ei) : mk(__int_as_float(0x7fc00000), 0.f);
+        }
     }
 
     // ---- release tensor memory
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(128));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
+                     "r"(128));
 }
 
 }  // namespace fl
