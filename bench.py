@@ -225,6 +225,57 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
     return out
 
 
+def multimode_measure(ctx, dev, B, steps, warmup):
+    """Config 4: B per-mode phase candidates φ ~ N(0, 1) (seeded) of the M = 10
+    HG(m+n<=3) problem on a 96x96 grid, Nt = 2^14 over 10 ps, L = 2 m, 5 nJ,
+    forward + band objective (red side beyond 2 THz) + adjoint + per-mode
+    gradient, one batched call on device buffers; and config 2 (M = 6,
+    Nt = 2^12 over 5 ps, 1 m, 2 nJ), one forward + adjoint."""
+    import torch
+    from fiberlab_gpu import problem as P
+    from fiberlab_gpu._capi import GPUProblem
+    out = {}
+    fp = P.multimode_problem(3, 96, 16384, 10.0, 2.0, 5e-9, 200e-15, seed=0,
+                             raman_threshold_thz=-2.0)
+    gp = GPUProblem(ctx, fp)
+    ph = np.random.default_rng(4).standard_normal((B, fp.M, fp.nt))
+    d_u0 = torch.from_numpy(np.ascontiguousarray(fp.uw0).view(np.float64).copy()).to(dev)
+    d_ph = torch.from_numpy(ph).to(dev)
+    d_m = torch.from_numpy(fp.mask.astype(np.uint8)).to(dev)
+    d_J = torch.empty(B, dtype=torch.float64, device=dev)
+    d_g = torch.empty((B, fp.M, fp.nt), dtype=torch.float64, device=dev)
+    run = lambda: gp.mode_phase_gradient_batch_device(d_u0.data_ptr(), B, d_ph.data_ptr(),
+                                                     d_m.data_ptr(), d_J.data_ptr(),
+                                                     d_g.data_ptr())
+    for _ in range(warmup):
+        run()
+    ms, st = [], None
+    for _ in range(steps):
+        st = run()
+        ms.append(ctx.timing()[0])
+    out["config4"] = {
+        "workload": f"config 4: M=10 HG(m+n<=3), Nt=2^14 over 10 ps, L=2 m, 5 nJ, {B} per-mode "
+                    "phase candidates N(0,1), fwd+adjoint, checkpoints 32 x 16",
+        "solves_per_s": B * steps / (sum(ms) / 1e3), "ms_per_batch": float(np.mean(ms)),
+        "steps_per_solve": {"forward": float(np.mean([s["naccept"] + s["nreject"] for s in st])),
+                            "adjoint": float(np.mean([s["adj_naccept"] + s["adj_nreject"]
+                                                      for s in st]))},
+        "contraction": "tcgen05 kind::tf32 (3xTF32) for the FP32 forward, DFMA for the adjoint"}
+    fp2 = P.multimode_problem(2, 64, 4096, 5.0, 1.0, 2e-9, 200e-15, seed=0,
+                              raman_threshold_thz=-2.0)
+    gp2 = GPUProblem(ctx, fp2)
+    lat = []
+    for i in range(4):
+        t = time.perf_counter()
+        gp2.phase_gradient_batch(np.zeros((1, fp2.nt)))
+        if i:
+            lat.append(1e3 * (time.perf_counter() - t))
+    out["config2"] = {"workload": "config 2: M=6 HG(m+n<=2), Nt=2^12 over 5 ps, L=1 m, 2 nJ, "
+                                  "one fwd+adjoint per call (host buffers)",
+                      "latency_ms_p50": float(np.median(lat))}
+    return out
+
+
 def init_dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -363,6 +414,10 @@ def run_ours(args):
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                "sample": f"{cores} problems of this workload, one per thread ({dt:.1f} s)"}
 
+    multimode = None
+    if args.mm_batch and rank == 0 and world == 1:
+        multimode = multimode_measure(ctx, dev, args.mm_batch, min(args.steps, 3), 1)
+
     serving = None
     if args.serve and rank == 0:
         serving = serving_measure(Context, local, args.serve, args.serve_plain)
@@ -383,6 +438,8 @@ def run_ours(args):
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
                 "plain_one_at_a_time": plain, "batched": batched_lat,
                 "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B}}
+        if multimode is not None:
+            line.update(multimode)
         if serving is not None:
             line["serving"] = serving
         print(json.dumps(line), flush=True)
@@ -399,6 +456,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="problems per GPU (default 4 x SMs)")
     ap.add_argument("--plain", type=int, default=8, help="one-at-a-time solves timed")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mm-batch", type=int, default=64,
+                    help="config-4 candidates per batch reported beside the headline (0: off)")
     ap.add_argument("--serve", type=int, default=0,
                     help="also run the config-3 serving stream with this many requests")
     ap.add_argument("--serve-plain", type=int, default=12,

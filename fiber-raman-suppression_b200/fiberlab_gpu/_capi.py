@@ -254,6 +254,15 @@ class GPUProblem:
             self.h, d_u0, B, d_phases, d_mask, int(log_cost), d_J, d_grad, st))
         return [s.as_dict() for s in st] if with_stats else None
 
+    def mode_phase_gradient_batch_device(self, d_u0: int, B: int, d_phases: int, d_mask: int,
+                                         d_J: int, d_grad: int, log_cost=False,
+                                         with_stats=True):
+        """Per-mode phases (B, M, Nt) and gradients on device buffers."""
+        st = (FlStats * B)() if with_stats else None
+        self.ctx.check(load().fl_mode_phase_gradient_batch_device(
+            self.h, d_u0, B, d_phases, d_mask, int(log_cost), d_J, d_grad, st))
+        return [s.as_dict() for s in st] if with_stats else None
+
     def close(self):
         if getattr(self, "h", None):
             load().fl_problem_destroy(self.h)
