@@ -140,13 +140,16 @@ def cpu_baseline(fp, nthreads: int, nprob: int):
     return nprob / dt, dt
 
 
-def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
+def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3, window_s=0.0):
     """Config-3 stream: n requests with Poisson arrivals at 2000/s, log2 Nt
     uniform on 11..15 over 10 ps, L ~ U(0.1, 5) m, P ~ U(0.02, 0.3) W, half
     forward-only and half forward + band gradient with phase N(0, 0.5²),
     through the continuous-batching server; then the first plain_n requests
     of the same stream one at a time through the plain entry points (a
-    problem per request, as the reference builds its tables per solve)."""
+    problem per request, as the reference builds its tables per solve).
+    With window_s > 0 both paths instead take the stream in arrival order for
+    window_s seconds and count the requests completed in that time (the
+    server's in-flight remainder is then abandoned)."""
     from fiberlab_gpu import problem as P
     from fiberlab_gpu._capi import FiberLabGPUError, GPUProblem
     from fiberlab_gpu.serving import Server
@@ -166,6 +169,8 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
     i, outstanding, t_last = 0, [], t0
     while i < n or outstanding:
         now = time.perf_counter() - t0
+        if window_s and now > window_s:
+            break
         while i < n and reqs[i].arrival_s <= now:
             r = reqs[i]
             fp, gp = grids[r.nt]
@@ -187,7 +192,7 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
             t_last = time.perf_counter()
         outstanding = still
         time.sleep(0.0005)
-    wall = t_last - t0
+    wall = window_s if window_s else t_last - t0
     info = srv.info()
     srv.close()
     done = statuses.get(0, 0)
@@ -203,10 +208,13 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
     pctx = ctx_cls(dev_index, checkpoints=256, segment_steps=128, step_log=32768,
                    max_iters=400000)
     tp, pdone = 0.0, 0
-    for r in reqs[:plain_n]:
+    for r in (reqs if window_s else reqs[:plain_n]):
+        if window_s and tp > window_s:
+            break
         fp0, _ = grids[r.nt]
         u0 = P.serving_launch(fp0, r.power_w)
         t = time.perf_counter()
+        ok = False
         try:
             fp = P.FiberProblem(**{**fp0.__dict__})
             fp.L = r.L
@@ -215,13 +223,21 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3):
                 gp.forward(u0)
             else:
                 gp.phase_gradient_batch(r.phase[None, :], u0=u0)
-            pdone += 1
+            ok = True
         except FiberLabGPUError:
             pass
         tp += time.perf_counter() - t
-    out["plain_one_at_a_time"] = {"requests": plain_n, "completed": pdone,
-                                  "solves_per_s": plain_n / tp, "total_s": tp}
-    out["speedup_vs_plain"] = out["solves_per_s"] / out["plain_one_at_a_time"]["solves_per_s"]
+        if ok and not (window_s and tp > window_s):  # finished inside the window
+            pdone += 1
+    if window_s:
+        out["window_s"] = window_s
+        out["plain_one_at_a_time"] = {"completed_in_window": pdone,
+                                      "solves_per_s": pdone / window_s}
+    else:
+        out["plain_one_at_a_time"] = {"requests": plain_n, "completed": pdone,
+                                      "solves_per_s": plain_n / tp, "total_s": tp}
+    ps = out["plain_one_at_a_time"]["solves_per_s"]
+    out["speedup_vs_plain"] = out["solves_per_s"] / ps if ps > 0 else None
     return out
 
 
@@ -420,7 +436,8 @@ def run_ours(args):
 
     serving = None
     if args.serve and rank == 0:
-        serving = serving_measure(Context, local, args.serve, args.serve_plain)
+        serving = serving_measure(Context, local, args.serve, args.serve_plain,
+                                  window_s=args.serve_window)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -460,6 +477,8 @@ def main():
                     help="config-4 candidates per batch reported beside the headline (0: off)")
     ap.add_argument("--serve", type=int, default=0,
                     help="also run the config-3 serving stream with this many requests")
+    ap.add_argument("--serve-window", type=float, default=0.0,
+                    help="seconds: count completions of both paths within this window")
     ap.add_argument("--serve-plain", type=int, default=12,
                     help="requests of that stream timed one at a time through the plain path")
     args = ap.parse_args()
