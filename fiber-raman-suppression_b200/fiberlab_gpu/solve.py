@@ -183,3 +183,86 @@ def phase_gradient(fp: P.FiberProblem, phases, *, log_cost=False, precision="fp3
         raise P.ArgumentError("fiber adjoint requires a fully permutation-symmetric gamma tensor")
     gp = GPUProblem(ctx or default_context(), fp, precision)
     return gp.phase_gradient_batch(phases, fp.mask, fp.uw0, log_cost)
+
+
+def _field_matrix(value, fp: P.FiberProblem, label: str):
+    """_field_matrix / _phase_matrix (physics_models.jl:685-731): a scalar, an
+    Nt vector (shared by the modes) or an (M, Nt) matrix, as (M, Nt) + shape."""
+    nt, M = fp.nt, fp.M
+    a = np.asarray(value, dtype=np.float64)
+    if a.ndim == 0:
+        if label == "phase":
+            raise P.ArgumentError("fiber field physics requires a vector or matrix decoded phase")
+        out, shape = np.full((M, nt), float(a)), "scalar"
+    elif a.ndim == 1:
+        if a.shape[0] != nt:
+            raise P.ArgumentError(f"{label} vector length {a.shape[0]} does not match Nt={nt}")
+        out, shape = np.repeat(a[None, :], M, axis=0), "vector"
+    elif a.ndim == 2:
+        if a.shape != (M, nt):
+            raise P.ArgumentError(f"{label} matrix size {a.shape[::-1]} does not match ({nt}, {M})")
+        out, shape = a.copy(), "matrix"
+    else:
+        raise P.ArgumentError(f"{label} must be a real scalar, vector, or matrix")
+    if not np.all(np.isfinite(out)):
+        raise P.ArgumentError(f"{label} values must be finite")
+    return out, shape
+
+
+def _for_shape(gradient: np.ndarray, shape: str):
+    """_physical_gradient_for_shape (physics_models.jl:732-737)."""
+    if shape == "scalar":
+        return np.array([gradient.sum()])
+    if shape == "vector":
+        return gradient.sum(axis=0)
+    return gradient
+
+
+def physical_gradient(fp: P.FiberProblem, control: dict, *, log_cost=False, precision="fp32",
+                      ctx: Context = None):
+    """Raman-band cost and the spectral-shaper physical gradient
+    (spectral_shaper_model, physics_models.jl:1021-1081): the launch
+    u_shaped = sqrt(energy) · amplitude · cis(phase) · uω0 (:791-797) runs
+    forward, the band objective (physics_helpers.jl:222-232, dB form :320-326)
+    seeds the adjoint, and from λ0 = λ(0)
+
+        ∂J/∂phase     = 2 Re(conj(λ0) i u_shaped)
+        ∂J/∂amplitude = 2 sqrt(energy) Re(conj(λ0) cis(phase) uω0)
+        ∂J/∂energy    = Re(Σ conj(λ0) u_shaped) / energy
+
+    each reduced to the shape of its control.  control may hold "phase",
+    "amplitude" and "energy"; returns (J, {name: gradient}) for those given."""
+    fp.validate()
+    if fp.mask is None or not np.any(fp.mask):
+        raise P.ArgumentError("band mask must contain at least one bin")
+    if not P.gamma_symmetric(fp.gamma):
+        raise P.ArgumentError("fiber adjoint requires a fully permutation-symmetric gamma tensor; "
+                              "use propagate(problem) for forward-only nonsymmetric models")
+    phase, phase_shape = _field_matrix(control.get("phase", np.zeros(fp.nt)), fp, "phase")
+    amplitude, amp_shape = _field_matrix(control.get("amplitude", 1.0), fp, "amplitude")
+    if not np.all(amplitude > 0):
+        raise P.ArgumentError("fiber field amplitude control must be strictly positive")
+    energy = float(control.get("energy", 1.0))
+    if not (np.isfinite(energy) and energy > 0):
+        raise P.ArgumentError("fiber field energy control must be positive and finite")
+    alpha = np.sqrt(energy)
+    shaped = alpha * amplitude * np.exp(1j * phase) * fp.uw0
+    if not (np.all(np.isfinite(shaped)) and np.linalg.norm(shaped) > 0):
+        raise P.ArgumentError("decoded controls must produce a finite, nonzero launch field")
+    gp = GPUProblem(ctx or default_context(), fp, precision)
+    out, _ = gp.forward(shaped)
+    J, seed = P.band_cost_and_seed(out[-1], fp.mask)
+    J, seed = P.maybe_log_cost(J, seed, log_cost)
+    lam0, _ = gp.adjoint(seed)
+    grads = {}
+    if "phase" in control:
+        grads["phase"] = _for_shape(2.0 * np.real(np.conj(lam0) * 1j * shaped), phase_shape)
+    if "amplitude" in control:
+        g = 2.0 * alpha * np.real(np.conj(lam0) * np.exp(1j * phase) * fp.uw0)
+        grads["amplitude"] = _for_shape(g, amp_shape)
+    if "energy" in control:
+        grads["energy"] = np.array([np.real(np.sum(np.conj(lam0) * shaped)) / energy])
+    for k, v in grads.items():
+        if not np.all(np.isfinite(v)):
+            raise P.ArgumentError(f"fiber field {k} physical gradient contains non-finite values")
+    return J, grads

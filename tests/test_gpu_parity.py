@@ -245,3 +245,33 @@ def test_status_codes_without_a_fault(gpu_ctx):
         GPUProblem(Context(0, checkpoints=2, segment_steps=1), long).phase_gradient_batch(
             np.zeros((1, long.nt)))
     assert e.value.status == 9
+
+
+def test_physical_gradient_phase_amplitude_energy(gpu_ctx):
+    # spectral_shaper_model's physical gradient (physics_models.jl:1021-1081):
+    # phase (vector), amplitude (vector) and energy controls of a 3-mode
+    # problem against the same chain rule applied to the oracle's λ0
+    from fiberlab_gpu import solve as S
+    fp = P.multimode_problem(1, 32, 512, 5.0, 0.4, 5e-9, 200e-15, seed=2,
+                             raman_threshold_thz=-5.0)
+    rng = np.random.default_rng(21)
+    control = {"phase": 0.3 * rng.standard_normal(fp.nt),
+               "amplitude": 1.0 + 0.1 * rng.standard_normal(fp.nt) ** 2,
+               "energy": 1.3}
+    J, g = S.physical_gradient(fp, control, ctx=gpu_ctx)
+    alpha = np.sqrt(control["energy"])
+    ph = np.repeat(control["phase"][None, :], fp.M, axis=0)
+    am = np.repeat(control["amplitude"][None, :], fp.M, axis=0)
+    shaped = alpha * am * np.exp(1j * ph) * fp.uw0
+    out, _, dense = O.forward(fp, u0=shaped, keep_dense=True)
+    Jo, seed = P.band_cost_and_seed(out[-1], fp.mask)
+    lam0, _ = O.adjoint(fp, dense, seed)
+    gp = (2 * np.real(np.conj(lam0) * 1j * shaped)).sum(axis=0)
+    ga = (2 * alpha * np.real(np.conj(lam0) * np.exp(1j * ph) * fp.uw0)).sum(axis=0)
+    ge = np.real(np.sum(np.conj(lam0) * shaped)) / control["energy"]
+    assert abs(10 * np.log10(J) - 10 * np.log10(Jo)) < DB_TOL
+    assert rel(g["phase"], gp) < GRAD_TOL
+    assert rel(g["amplitude"], ga) < GRAD_TOL
+    assert abs(g["energy"][0] - ge) <= GRAD_TOL * abs(ge)
+    with pytest.raises(P.ArgumentError):
+        S.physical_gradient(fp, {"amplitude": -1.0}, ctx=gpu_ctx)
