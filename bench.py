@@ -292,6 +292,18 @@ def multimode_measure(ctx, dev, B, steps, warmup):
     return out
 
 
+def max_over_ranks(value: float, device=None) -> float:
+    """The job's time: the maximum of a per-rank value over all ranks (one
+    all-reduce; the identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def init_dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -380,12 +392,7 @@ def run_ours(args):
         dist.barrier()
     clocks = sampler.stop()
     t_rank = sum(call_ms)
-    if world > 1:
-        tt = torch.tensor([t_rank], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_job = float(tt.item())
-    else:
-        t_job = t_rank
+    t_job = max_over_ranks(t_rank, dev)
     value = B * args.steps * world / (t_job / 1e3)
 
     # roofline of the stepper kernel: algorithmic bytes per launch / launch time
