@@ -29,9 +29,8 @@ def cfg0(nt=8192, T=10.0, **kw):
 @pytest.mark.parametrize("nt", [64, 256, 1024, 8192, 16384, 32768])
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_rhs_matches_oracle(gpu_ctx, nt, precision):
-    # 2^15 runs on the cluster transform of the multimode runtime (4 CTAs)
-    if precision == "fp64" and nt == 16384:
-        pytest.skip("FP64 mode is built up to 2^13 on one CTA, and at 2^15 on a cluster")
+    # FP64 mode beyond 2^13 and both modes at 2^15 run on the multimode
+    # runtime's kernels (2^15 through a 4-CTA cluster transform)
     fp = P.single_mode_problem(nt=nt, time_window_ps=10.0 if nt >= 1024 else 3.0, L=0.5,
                                power_w=0.1, rep_rate_hz=80.5e6, validate_grid=False)
     rng = np.random.default_rng(nt)
@@ -124,6 +123,19 @@ def test_fp64_mode_matches_oracle(gpu_ctx, nt, T):
     ref, rst, _ = O.forward(fp)
     assert rel(out[-1], ref[-1]) < FIELD_TOL_FP64
     assert st["naccept"] == rst["naccept"]
+
+
+@pytest.mark.parametrize("nt", [16384, 32768])
+def test_fp64_mode_large_grids(gpu_ctx, nt):
+    # FP64 mode beyond one CTA's transform: the same steps as the oracle
+    # (equal accepted count) and the field to FP64 round-off over 5 cm
+    fp = P.single_mode_problem(nt=nt, time_window_ps=10.0, L=0.05, power_w=0.1,
+                               rep_rate_hz=80.5e6, validate_grid=False)
+    out, st = GPUProblem(gpu_ctx, fp, "fp64").forward()
+    ref, rst, _ = O.forward(fp)
+    assert st["status"] == 0 and st["z_end"] == fp.L
+    assert st["naccept"] == rst["naccept"]
+    assert rel(out[-1], ref[-1]) < 1e-9
 
 
 def test_saveat_dense_output(gpu_ctx):

@@ -116,3 +116,35 @@ def test_serving_wait_timeout_then_result(gpu_ctx):
     srv.wait(h)
     assert h.status == 0 and h.stats["adj_naccept"] > 0
     srv.close()
+
+
+def test_serving_multimode_requests(gpu_ctx):
+    # a 3-mode forward and band gradient beside a single-mode forward in one
+    # server: the multimode requests run on the mode-parallel kernels in
+    # their own bucket, with the same answers as the plain entry points
+    fp = P.multimode_problem(1, 32, 512, 5.0, 0.3, 4e-9, 200e-15, seed=4,
+                             raman_threshold_thz=-5.0)
+    gp = GPUProblem(gpu_ctx, fp)
+    sm = P.serving_grid_problem(2048)
+    gsm = GPUProblem(gpu_ctx, sm)
+    phi = 0.4 * np.random.default_rng(2).standard_normal(fp.nt)
+    srv = Server(gpu_ctx)
+    hf = srv.submit_forward(gp, L=0.2)
+    hg = srv.submit_band_gradient(gp, phi, L=0.2)
+    hs = srv.submit_forward(gsm, u0=P.serving_launch(sm, 0.1), L=0.3)
+    for h in (hf, hg, hs):
+        srv.wait(h)
+        assert h.status == 0
+    short = P.FiberProblem(**{**fp.__dict__})
+    short.L = 0.2
+    gshort = GPUProblem(gpu_ctx, short)
+    out, _ = gshort.forward()
+    assert np.array_equal(out[-1], hf.out_field)
+    J, g, _ = gshort.phase_gradient_batch(phi[None, :])
+    assert abs(J[0] - hg.J) <= 1e-9 * abs(J[0])
+    assert rel(hg.out_grad, g[0]) < GRAD_TOL
+    smL = P.FiberProblem(**{**sm.__dict__})
+    smL.L = 0.3
+    out_sm, _ = GPUProblem(gpu_ctx, smL).forward(P.serving_launch(sm, 0.1))
+    assert np.array_equal(out_sm[-1], hs.out_field)
+    srv.close()
