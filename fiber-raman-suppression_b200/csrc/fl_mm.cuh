@@ -249,8 +249,13 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
         const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
         const double zz = st.ezload;
         const double* lg = d.steplog;
-        int n = seg_lo;
-        while (n + 1 < seg_hi && lg[2 * (n + 1)] <= zz) n++;
+        // last stored step starting at or before zz, by bisection
+        int n = seg_lo, hi = seg_hi - 1;
+        while (n < hi) {
+            const int mid = (n + hi + 1) >> 1;
+            if (lg[2 * mid] <= zz) n = mid;
+            else hi = mid - 1;
+        }
         const double zn = lg[2 * n], dtn = lg[2 * n + 1];
         const double th = (zz - zn) / dtn, t2 = th * th, t3 = t2 * th, t4 = t3 * th;
         const size_t base = (size_t)(n - seg_lo) * 5 * NM;

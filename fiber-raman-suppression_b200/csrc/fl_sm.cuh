@@ -153,6 +153,24 @@ __device__ __forceinline__ void load_twiddles(const SlotDesc& d, double* red) {
     __syncthreads();
 }
 
+// The field handed between the state machine and the out-of-line RHS, as
+// element s = bin t + T s of thread t: in the transform buffer in shared
+// memory where that buffer holds a complex FP64 field (Nt <= 2^13), else in
+// a per-thread array in local memory.  Each thread only touches its own
+// bins, so handing over needs no barrier; the RHS synchronises once after
+// reading its input, before its first transform exchange overwrites the
+// buffer.
+template <typename C, int LOGN, int LOGE>
+struct FieldIO {
+    static constexpr bool SMEM = !SmemPlan<double, LOGN>::SPLIT;
+    static constexpr int T = FftShape<LOGN, LOGE>::T;
+    C* p;
+    __device__ __forceinline__ C& operator[](int s) const {
+        if constexpr (SMEM) return p[pad(threadIdx.x + T * s)];
+        else return p[s];
+    }
+};
+
 // Block-level pieces of one problem's solve in RHS precision R.
 template <typename R, int LOGN, int LOGE>
 struct SmSolver {
@@ -160,6 +178,7 @@ struct SmSolver {
     static constexpr int N = S::N, E = S::E, T = S::T;
     static constexpr int P = sizeof(R) == 8 ? 1 : 0;  // table precision index
     using C = cx<R>;
+    using IO = FieldIO<C, LOGN, LOGE>;
 
     const SlotDesc& d;
     void* sm;       // padded transform buffer
@@ -280,21 +299,40 @@ struct SmSolver {
         return (C*)k[p];
     }
 
+    // Stage combinations read the stage vectors stage-outer and point-inner:
+    // each thread issues the loads of SC of its points for one stage
+    // together, so SC loads are in flight per thread instead of one.  The
+    // per-point summation order (stage 0 first) is unchanged.
+    static constexpr int SC = E < 8 ? E : 8;                      // points per chunk
+    static constexpr int SC7 = E < 8 ? E : (sizeof(R) == 8 ? 4 : 8);  // stage 7: two sums
+    static_assert(E % SC == 0 && E % SC7 == 0, "chunks tile the thread's points");
+
     // v = ũ_n + dt Σ_{j<st} a[st][j] k_j   (FP64 accumulation)
     __device__ __forceinline__ void stage_input(int st, const double* u, void* const (&k)[7],
-                                                int perm, double dt, C (&v)[E]) {
+                                                int perm, double dt, IO v) {
 #pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            double ar = 0.0, ai = 0.0;
+        for (int s0 = 0; s0 < E; s0 += SC) {
+            double ar[SC], ai[SC];
+#pragma unroll
+            for (int c = 0; c < SC; c++) ar[c] = ai[c] = 0.0;
+#pragma unroll 1
             for (int j = 0; j < st; j++) {
-                const C kj = kp(k, perm, j)[b];
+                const C* __restrict__ kj = kp(k, perm, j);
                 const double a = kT5a[st][j];
-                ar += a * (double)kj.re;
-                ai += a * (double)kj.im;
+                C x[SC];
+#pragma unroll
+                for (int c = 0; c < SC; c++) x[c] = kj[bin(s0 + c)];
+#pragma unroll
+                for (int c = 0; c < SC; c++) {
+                    ar[c] += a * (double)x[c].re;
+                    ai[c] += a * (double)x[c].im;
+                }
             }
-            const cx<double> un = ld2(u, b);
-            v[s] = mk((R)(un.re + dt * ar), (R)(un.im + dt * ai));
+#pragma unroll
+            for (int c = 0; c < SC; c++) {
+                const cx<double> un = ld2(u, bin(s0 + c));
+                v[s0 + c] = mk((R)(un.re + dt * ar[c]), (R)(un.im + dt * ai[c]));
+            }
         }
     }
 
@@ -302,35 +340,47 @@ struct SmSolver {
     // dt Σ_{j<7} b̃_j k_j and the weights abstol + reltol max(|u_n|,|u_{n+1}|)
     __device__ __forceinline__ void stage7_input(const double* u, double* unew,
                                                  void* const (&k)[7], int perm, double dt,
-                                                 double abstol, double reltol, C (&v)[E],
+                                                 double abstol, double reltol, IO v,
                                                  bool want_err) {
 #pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int b = bin(s);
-            double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
+        for (int s0 = 0; s0 < E; s0 += SC7) {
+            double ar[SC7], ai[SC7], er[SC7], ei[SC7];
+#pragma unroll
+            for (int c = 0; c < SC7; c++) ar[c] = ai[c] = er[c] = ei[c] = 0.0;
+#pragma unroll 1
             for (int j = 0; j < 6; j++) {
-                const C kj = kp(k, perm, j)[b];
+                const C* __restrict__ kj = kp(k, perm, j);
                 const double a = kT5a[6][j], bt = kT5bt[j];
-                ar += a * (double)kj.re;
-                ai += a * (double)kj.im;
-                er += bt * (double)kj.re;
-                ei += bt * (double)kj.im;
+                C x[SC7];
+#pragma unroll
+                for (int c = 0; c < SC7; c++) x[c] = kj[bin(s0 + c)];
+#pragma unroll
+                for (int c = 0; c < SC7; c++) {
+                    ar[c] += a * (double)x[c].re;
+                    ai[c] += a * (double)x[c].im;
+                    er[c] += bt * (double)x[c].re;
+                    ei[c] += bt * (double)x[c].im;
+                }
             }
-            const cx<double> un = ld2(u, b);
-            const cx<double> u1 = mk(un.re + dt * ar, un.im + dt * ai);
-            st2(unew, b, u1);
-            if (want_err) {
-                st2(d.esv, b, mk(dt * er, dt * ei));
-                const double m0 = sqrt(un.re * un.re + un.im * un.im);
-                const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
-                d.skv[b] = abstol + fmax(m0, m1) * reltol;
+#pragma unroll
+            for (int c = 0; c < SC7; c++) {
+                const int b = bin(s0 + c);
+                const cx<double> un = ld2(u, b);
+                const cx<double> u1 = mk(un.re + dt * ar[c], un.im + dt * ai[c]);
+                st2(unew, b, u1);
+                if (want_err) {
+                    st2(d.esv, b, mk(dt * er[c], dt * ei[c]));
+                    const double m0 = sqrt(un.re * un.re + un.im * un.im);
+                    const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
+                    d.skv[b] = abstol + fmax(m0, m1) * reltol;
+                }
+                v[s0 + c] = down<R>(u1);
             }
-            v[s] = down<R>(u1);
         }
     }
 
     // finish the error estimate with k7 (in v) -> EEst (block-uniform)
-    __device__ __forceinline__ double error_norm(const C (&k7)[E], double dt) {
+    __device__ __forceinline__ double error_norm(IO k7, double dt) {
         const double bt7 = kT5bt[6];
         double acc = 0.0;
 #pragma unroll
@@ -411,9 +461,16 @@ struct SegLoader {
                 w[s] = down<R>(ld2(direct, threadIdx.x + FftShape<LOGN, LOGE>::T * s));
             return;
         }
+        // the last stored step of the segment starting at or before zz (the
+        // logged step starts increase): a bisection, so a long segment costs
+        // log2(length) dependent loads instead of one per step
         const double* lg = d.steplog;
-        int n = seg_lo;
-        while (n + 1 < seg_hi && lg[2 * (n + 1)] <= zz) n++;
+        int n = seg_lo, hi = seg_hi - 1;
+        while (n < hi) {
+            const int mid = (n + hi + 1) >> 1;
+            if (lg[2 * mid] <= zz) n = mid;
+            else hi = mid - 1;
+        }
         const double zn = lg[2 * n], dtn = lg[2 * n + 1];
         interp_step<RF, R, LOGN, LOGE>(d, n - seg_lo, dtn, (zz - zn) / dtn, w);
     }
@@ -424,12 +481,13 @@ struct SegLoader {
 // values; the 2E-register field crosses the call through local memory.
 template <typename R, int LOGN, int LOGE>
 __device__ __noinline__ void rhs_fwd_call(const SlotDesc* d, void* sm, double* red, double z,
-                                          cx<R>* vio) {
+                                          FieldIO<cx<R>, LOGN, LOGE> vio) {
     using Sol = SmSolver<R, LOGN, LOGE>;
     Sol S(*d, sm, red);
     cx<R> v[Sol::E];
 #pragma unroll
     for (int s = 0; s < Sol::E; s++) v[s] = vio[s];
+    if constexpr (FieldIO<cx<R>, LOGN, LOGE>::SMEM) __syncthreads();
     S.rhs(false, z, v, [](cx<R>(&)[Sol::E]) {});
 #pragma unroll
     for (int s = 0; s < Sol::E; s++) vio[s] = v[s];
@@ -437,13 +495,14 @@ __device__ __noinline__ void rhs_fwd_call(const SlotDesc* d, void* sm, double* r
 
 template <typename RF, typename R, int LOGN, int LOGE>
 __device__ __noinline__ void rhs_adj_call(const SlotDesc* d, void* sm, double* red, double z,
-                                          cx<R>* vio, int seg_lo, int seg_hi, double zload,
-                                          const double* ufwd) {
+                                          FieldIO<cx<R>, LOGN, LOGE> vio, int seg_lo, int seg_hi,
+                                          double zload, const double* ufwd) {
     using Sol = SmSolver<R, LOGN, LOGE>;
     Sol S(*d, sm, red);
     cx<R> v[Sol::E];
 #pragma unroll
     for (int s = 0; s < Sol::E; s++) v[s] = vio[s];
+    if constexpr (FieldIO<cx<R>, LOGN, LOGE>::SMEM) __syncthreads();
     SegLoader<RF, R, LOGN, LOGE> ld{*d, seg_lo, seg_hi, zload, ufwd};
     S.rhs(true, z, v, ld);
 #pragma unroll
@@ -471,14 +530,18 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     double* red = reinterpret_cast<double*>(smraw + SmemPlan<RA, LOGN>::BYTES);
     load_twiddles<LOGN>(*d, red);
     if (adjoint) {
-        cx<RA> v[S::E];
+        using IO = FieldIO<cx<RA>, LOGN, LOGE>;
+        cx<RA> vl[IO::SMEM ? 1 : S::E];
+        const IO v{IO::SMEM ? reinterpret_cast<cx<RA>*>(smraw) : vl};
 #pragma unroll
         for (int s = 0; s < S::E; s++) v[s] = down<RA>(ld2(in, threadIdx.x + S::T * s));
         rhs_adj_call<RF, RA, LOGN, LOGE>(d, smraw, red, z, v, 0, 0, 0.0, ufwd);
 #pragma unroll
         for (int s = 0; s < S::E; s++) st2(out, threadIdx.x + S::T * s, up(v[s]));
     } else {
-        cx<RF> v[S::E];
+        using IO = FieldIO<cx<RF>, LOGN, LOGE>;
+        cx<RF> vl[IO::SMEM ? 1 : S::E];
+        const IO v{IO::SMEM ? reinterpret_cast<cx<RF>*>(smraw) : vl};
 #pragma unroll
         for (int s = 0; s < S::E; s++) v[s] = down<RF>(ld2(in, threadIdx.x + S::T * s));
         rhs_fwd_call<RF, LOGN, LOGE>(d, smraw, red, z, v);
@@ -507,7 +570,8 @@ __device__ __forceinline__ void restore_checkpoint(const SlotDesc& d, int seg, S
 // Hairer initial step, part 1 (after f0): stores f0 as the FSAL derivative,
 // returns the probe step dt0 (> 0) or, when no probe is needed, -dtinit.
 template <typename K, int LOGN, int LOGE>
-__device__ __forceinline__ double init_after_f0(const double* x0, cx<K>* k1, const cx<K>* v,
+__device__ __forceinline__ double init_after_f0(const double* x0, cx<K>* k1,
+                                                FieldIO<cx<K>, LOGN, LOGE> v,
                                                 double at, double rt, double L, double dtmin,
                                                 double* red, double& d1_out) {
     using S = FftShape<LOGN, LOGE>;
@@ -535,7 +599,8 @@ __device__ __forceinline__ double init_after_f0(const double* x0, cx<K>* k1, con
 
 // Hairer initial step, part 2 (after the probe f1 at x0 ± dt0 f0)
 template <typename K, int LOGN, int LOGE>
-__device__ __forceinline__ double init_after_f1(const double* x0, const cx<K>* k1, const cx<K>* v,
+__device__ __forceinline__ double init_after_f1(const double* x0, const cx<K>* k1,
+                                                FieldIO<cx<K>, LOGN, LOGE> v,
                                                 double at, double rt, double dt0, double d1,
                                                 double L, double dtmin, double* red) {
     using S = FftShape<LOGN, LOGE>;
@@ -580,8 +645,12 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     SolA SA(d, smraw, red);
     const int tid = threadIdx.x;
     const double L = d.L, dtmin = kEps * L;
-    CF vf[E];
-    CA va[E];
+    using IOF = FieldIO<CF, LOGN, LOGE>;
+    using IOA = FieldIO<CA, LOGN, LOGE>;
+    CF vfl[IOF::SMEM ? 1 : E];  // local-memory field (Nt = 2^14 only)
+    CA val[IOA::SMEM ? 1 : E];
+    const IOF vf{IOF::SMEM ? reinterpret_cast<CF*>(smraw) : vfl};
+    const IOA va{IOA::SMEM ? reinterpret_cast<CA*>(smraw) : val};
     int evals = 0;
 
     while (st.phase != PH_DONE && evals < max_evals) {
@@ -866,22 +935,39 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double* u = d.u[st.cur];
             if (rec) {
                 // interpolant of this step: c0 = ũ_n, c_p = Σ_i r_ip k_i
+                // (stage-outer over chunks of 4 points, as in stage_input)
                 CF* sg = (CF*)d.seg + (size_t)st.rec_pos * 5 * N;
+                constexpr int RC = E < 4 ? E : 4;
+                static_assert(E % RC == 0, "chunks tile the thread's points");
 #pragma unroll
-                for (int s = 0; s < E; s++) {
-                    const int b = SolF::bin(s);
-                    sg[b] = down<RF>(ld2(u, b));
-                    double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+                for (int s0 = 0; s0 < E; s0 += RC) {
+                    double cr[RC][4], ci[RC][4];
+#pragma unroll
+                    for (int c = 0; c < RC; c++)
+#pragma unroll
+                        for (int q = 0; q < 4; q++) cr[c][q] = ci[c][q] = 0.0;
+#pragma unroll 1
                     for (int i = 0; i < 7; i++) {
-                        const CF ki = SolF::kp(d.kf, st.kperm, i)[b];
+                        const CF* __restrict__ kv = SolF::kp(d.kf, st.kperm, i);
+                        CF x[RC];
 #pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            cr[q] += kT5r[i][q] * (double)ki.re;
-                            ci[q] += kT5r[i][q] * (double)ki.im;
-                        }
+                        for (int c = 0; c < RC; c++) x[c] = kv[SolF::bin(s0 + c)];
+#pragma unroll
+                        for (int c = 0; c < RC; c++)
+#pragma unroll
+                            for (int q = 0; q < 4; q++) {
+                                cr[c][q] += kT5r[i][q] * (double)x[c].re;
+                                ci[c][q] += kT5r[i][q] * (double)x[c].im;
+                            }
                     }
 #pragma unroll
-                    for (int q = 0; q < 4; q++) sg[(q + 1) * N + b] = mk((RF)cr[q], (RF)ci[q]);
+                    for (int c = 0; c < RC; c++) {
+                        const int b = SolF::bin(s0 + c);
+                        sg[b] = down<RF>(ld2(u, b));
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            sg[(q + 1) * N + b] = mk((RF)cr[c][q], (RF)ci[c][q]);
+                    }
                 }
                 st.cur ^= 1;
                 st.kperm ^= 1;
