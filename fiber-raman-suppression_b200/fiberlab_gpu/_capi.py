@@ -220,14 +220,22 @@ class GPUProblem:
                                           None if uf is None else _ptr(uf), _ptr(out)))
         return out
 
-    def phase_gradient_batch(self, phases, mask=None, u0=None, log_cost=False):
+    def phase_gradient_batch(self, phases, mask=None, u0=None, log_cost=False, out=None):
+        """Host-buffer batch: phases (B, Nt) -> J (B,), grad (B, Nt).  out =
+        (J, grad) reuses caller arrays (page-locked ones make the library's
+        copies direct transfers)."""
         fp = self.fp
         ph = np.ascontiguousarray(np.atleast_2d(phases), dtype=np.float64)
         B = ph.shape[0]
         u0 = np.ascontiguousarray(fp.uw0 if u0 is None else u0, dtype=np.complex128)
         m = np.ascontiguousarray(fp.mask if mask is None else mask, dtype=np.uint8)
-        J = np.empty(B)
-        g = np.empty((B, fp.nt))
+        if out is None:
+            J, g = np.empty(B), np.empty((B, fp.nt))
+        else:
+            J, g = out
+            if J.shape != (B,) or g.shape != (B, fp.nt) or J.dtype != np.float64 or \
+                    g.dtype != np.float64 or not (J.flags.c_contiguous and g.flags.c_contiguous):
+                raise ValueError("out must be contiguous float64 arrays of shapes (B,), (B, Nt)")
         st = (FlStats * B)()
         self.ctx.check(load().fl_phase_gradient_batch(self.h, _ptr(u0), B, _ptr(ph), _ptr(m),
                                                       int(log_cost), _ptr(J), _ptr(g), st))

@@ -21,6 +21,7 @@ from typing import Optional
 
 import numpy as np
 
+from . import objectives as O
 from . import problem as P
 from ._capi import Context, GPUProblem
 
@@ -219,12 +220,15 @@ def _for_shape(gradient: np.ndarray, shape: str):
 
 
 def physical_gradient(fp: P.FiberProblem, control: dict, *, log_cost=False, precision="fp32",
-                      ctx: Context = None):
-    """Raman-band cost and the spectral-shaper physical gradient
+                      ctx: Context = None, objective: str = "raman_band",
+                      worst_mode_tau: float = 50.0):
+    """Objective cost and the spectral-shaper physical gradient
     (spectral_shaper_model, physics_models.jl:1021-1081): the launch
     u_shaped = sqrt(energy) · amplitude · cis(phase) · uω0 (:791-797) runs
-    forward, the band objective (physics_helpers.jl:222-232, dB form :320-326)
-    seeds the adjoint, and from λ0 = λ(0)
+    forward on the GPU, the named field objective (objectives.NAMES: the
+    Raman band by default, physics_helpers.jl:222-318, dB form :320-326)
+    gives J and the seed λ(L) on the host, the adjoint runs on the GPU, and
+    from λ0 = λ(0)
 
         ∂J/∂phase     = 2 Re(conj(λ0) i u_shaped)
         ∂J/∂amplitude = 2 sqrt(energy) Re(conj(λ0) cis(phase) uω0)
@@ -233,7 +237,8 @@ def physical_gradient(fp: P.FiberProblem, control: dict, *, log_cost=False, prec
     each reduced to the shape of its control.  control may hold "phase",
     "amplitude" and "energy"; returns (J, {name: gradient}) for those given."""
     fp.validate()
-    if fp.mask is None or not np.any(fp.mask):
+    cost_fn = O.objective(objective, fp.mask, fp.sim, worst_mode_tau)
+    if objective != "temporal_width" and (fp.mask is None or not np.any(fp.mask)):
         raise P.ArgumentError("band mask must contain at least one bin")
     if not P.gamma_symmetric(fp.gamma):
         raise P.ArgumentError("fiber adjoint requires a fully permutation-symmetric gamma tensor; "
@@ -251,8 +256,7 @@ def physical_gradient(fp: P.FiberProblem, control: dict, *, log_cost=False, prec
         raise P.ArgumentError("decoded controls must produce a finite, nonzero launch field")
     gp = GPUProblem(ctx or default_context(), fp, precision)
     out, _ = gp.forward(shaped)
-    J, seed = P.band_cost_and_seed(out[-1], fp.mask)
-    J, seed = P.maybe_log_cost(J, seed, log_cost)
+    J, seed = P.maybe_log_cost(*cost_fn(out[-1]), log_cost)
     lam0, _ = gp.adjoint(seed)
     grads = {}
     if "phase" in control:

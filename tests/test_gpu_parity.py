@@ -287,3 +287,24 @@ def test_physical_gradient_phase_amplitude_energy(gpu_ctx):
     assert abs(g["energy"][0] - ge) <= GRAD_TOL * abs(ge)
     with pytest.raises(P.ArgumentError):
         S.physical_gradient(fp, {"amplitude": -1.0}, ctx=gpu_ctx)
+
+
+@pytest.mark.parametrize("objective", ["fundamental_mode", "worst_mode", "raman_peak",
+                                       "temporal_width"])
+def test_physical_gradient_objectives(gpu_ctx, objective):
+    # the other field objectives of the reference registry
+    # (physics_helpers.jl:234-318): GPU forward, host seed, GPU adjoint,
+    # against the same seed through the oracle's forward and adjoint
+    from fiberlab_gpu import objectives as Ob
+    from fiberlab_gpu import solve as S
+    fp = P.multimode_problem(1, 32, 512, 5.0, 0.4, 5e-9, 200e-15, seed=2,
+                             raman_threshold_thz=-3.0)
+    phi = 0.3 * np.random.default_rng(31).standard_normal(fp.nt)
+    J, g = S.physical_gradient(fp, {"phase": phi}, ctx=gpu_ctx, objective=objective)
+    shaped = np.exp(1j * phi)[None, :] * fp.uw0
+    out, _, dense = O.forward(fp, u0=shaped, keep_dense=True)
+    Jo, seed = Ob.cost_and_seed(objective, out[-1], fp.mask, fp.sim)
+    lam0, _ = O.adjoint(fp, dense, seed)
+    go = (2 * np.real(np.conj(lam0) * 1j * shaped)).sum(axis=0)
+    assert abs(J - Jo) <= 1e-4 * abs(Jo)
+    assert rel(g["phase"], go) < GRAD_TOL
