@@ -319,7 +319,8 @@ def single_mode_problem(nt: int = 8192, time_window_ps: float = 10.0, L: float =
                         hR=raman["hRω"], one_m_fR=raman["one_m_fR"], L=float(L), uw0=uw0,
                         reltol=reltol, abstol=abstol,
                         mask=band_mask(sim, raman_threshold_thz),
-                        meta=dict(kind="single_mode", power_w=power_w))
+                        meta=dict(kind="single_mode", power_w=power_w, fwhm_s=fwhm_s,
+                                  rep_rate_hz=rep_rate_hz))
 
 
 def hg_group(m: int, n: int) -> int:
@@ -359,7 +360,8 @@ def multimode_problem(max_order: int, nx: int, nt: int, time_window_ps: float, L
     return FiberProblem(sim=sim, D=D, gamma=gam, hR=raman["hRω"],
                         one_m_fR=raman["one_m_fR"], L=float(L), uw0=uw0, reltol=reltol,
                         abstol=abstol, mask=band_mask(sim, raman_threshold_thz),
-                        meta=dict(kind="multimode", modes=idx, launch=launch, dx=dx))
+                        meta=dict(kind="multimode", modes=idx, launch=launch, dx=dx,
+                                  fwhm_s=fwhm_s))
 
 
 # ---------------------------------------------------------------------------

@@ -6,6 +6,7 @@ error behaviour:
   solve_disp_mmf(uω0, fiber, sim)            src/simulation/simulate_disp_mmf.jl:183-207
   solve_adjoint_disp_mmf(λωL, ũω, fiber, sim) src/simulation/sensitivity_disp_mmf.jl:309-332
   propagate(problem; saveat)                 src/fiberlab/propagation.jl:89-123
+  metrics(result), verify(result; ...)       src/fiberlab/propagation.jl:176-304
   physical phase gradient                    src/fiberlab/physics_models.jl:1033-1046
 
 `fiber` and `sim` are the reference's dictionaries (keys "Dω", "γ", "hRω",
@@ -142,6 +143,7 @@ class PropagationResult:
     output_spectrum: np.ndarray
     accepted_steps: int
     rhs_evaluations: int
+    problem: Optional[P.FiberProblem] = None
 
 
 def save_positions(saveat, length_m: float) -> np.ndarray:
@@ -171,7 +173,145 @@ def propagate(fp: P.FiberProblem, saveat=None, *, precision="fp32",
     spectra, stats = gp.forward(fp.uw0, z)
     return PropagationResult(z_m=z, spectra=spectra, input_spectrum=spectra[0].copy(),
                              output_spectrum=spectra[-1].copy(),
-                             accepted_steps=stats["naccept"], rhs_evaluations=stats["nf"])
+                             accepted_steps=stats["naccept"], rhs_evaluations=stats["nf"],
+                             problem=fp)
+
+
+# ---------------------------------------------------------------------------
+# Evidence over the saved spectra (propagation.jl:176-304): FP64 reductions
+# of the lab-frame samples the GPU forward returned.
+
+def edge_fraction(power: np.ndarray) -> float:
+    """_edge_fraction (propagation.jl:176-182): power in the first and last
+    max(1, floor(0.05 n)) samples over the total."""
+    power = np.asarray(power, dtype=np.float64)
+    k = max(1, int(np.floor(0.05 * power.shape[0])))
+    total = float(np.sum(power))
+    if not total > 0:
+        raise P.ArgumentError("field power must be nonzero")
+    return float((np.sum(power[:k]) + np.sum(power[-k:])) / total)
+
+
+def field_metrics(spectrum: np.ndarray, sim: dict) -> dict:
+    """_field_metrics (propagation.jl:189-202) of one (M, Nt) spectrum: the
+    time-domain field is fft along time (the reference's convention)."""
+    u = np.atleast_2d(np.asarray(spectrum, dtype=np.complex128))
+    temporal = np.fft.fft(u, axis=1)
+    tpow = np.sum(np.abs(temporal) ** 2, axis=0)
+    mode_energy = np.sum(np.abs(temporal) ** 2, axis=1) * float(sim["Δt"])
+    spow = np.fft.fftshift(np.sum(np.abs(u) ** 2, axis=0))
+    return {"energy_pj": float(np.sum(mode_energy)), "mode_energy_pj": mode_energy,
+            "peak_power_w": float(np.max(tpow)),
+            "temporal_edge_fraction": edge_fraction(tpow),
+            "spectral_edge_fraction": edge_fraction(spow),
+            "photon_number": P.photon_number(u, sim)}
+
+
+def _integrity(result: PropagationResult) -> bool:
+    """The structural part of _propagation_integrity (propagation.jl:125-145):
+    sizes, ordered finite positions from 0 to L, and the input/output samples
+    matching the first/last spectra and the problem's launch.  (The
+    reference's SHA-256 evidence seal is provenance bookkeeping outside the
+    solver path.)"""
+    try:
+        fp = result.problem
+        z = np.asarray(result.z_m, dtype=np.float64)
+        return (fp is not None and z.ndim == 1 and len(z) >= 2 and
+                result.spectra.shape == (len(z), fp.M, fp.nt) and
+                bool(np.all(np.isfinite(z))) and bool(np.all(np.diff(z) > 0)) and
+                z[0] == 0.0 and z[-1] == float(fp.L) and
+                np.array_equal(result.input_spectrum, fp.uw0) and
+                np.array_equal(result.input_spectrum, result.spectra[0]) and
+                np.array_equal(result.output_spectrum, result.spectra[-1]) and
+                result.accepted_steps >= 0 and result.rhs_evaluations >= 0)
+    except (AttributeError, TypeError, ValueError):
+        return False
+
+
+def _propagation_metrics(result: PropagationResult) -> dict:
+    """_propagation_metrics (propagation.jl:204-237)."""
+    fp = result.problem
+    samples = [field_metrics(result.spectra[i], fp.sim) for i in range(len(result.z_m))]
+    inp, out = samples[0], samples[-1]
+    energy_drift = np.array([s["energy_pj"] / inp["energy_pj"] - 1 for s in samples])
+    photon_drift = np.array([s["photon_number"] / inp["photon_number"] - 1 for s in samples])
+    fwhm = fp.meta.get("fwhm_s") if fp.meta else None
+    launch = None if fwhm is None else fwhm * 1e12 / float(fp.sim["Δt"])
+    return {
+        "samples": fp.nt, "modes": fp.M, "saved_positions": len(result.z_m),
+        "length_m": float(fp.L), "time_window_ps": float(fp.sim["time_window"]),
+        "delta_t_ps": float(fp.sim["Δt"]),
+        "frequency_spacing_thz": 1.0 / float(fp.sim["time_window"]),
+        "input_energy_pj": inp["energy_pj"], "output_energy_pj": out["energy_pj"],
+        "input_mode_energy_pj": inp["mode_energy_pj"],
+        "output_mode_energy_pj": out["mode_energy_pj"],
+        "relative_energy_change": float(energy_drift[-1]),
+        "max_relative_energy_change": float(np.max(np.abs(energy_drift))),
+        "input_peak_power_w": inp["peak_power_w"], "output_peak_power_w": out["peak_power_w"],
+        "max_temporal_edge_fraction": max(s["temporal_edge_fraction"] for s in samples),
+        "max_spectral_edge_fraction": max(s["spectral_edge_fraction"] for s in samples),
+        "max_photon_number_drift": float(np.max(np.abs(photon_drift))),
+        "launch_samples_per_fwhm": launch, "retcode": "Success",
+        "accepted_steps": result.accepted_steps, "rhs_evaluations": result.rhs_evaluations,
+    }
+
+
+def metrics(result: PropagationResult) -> dict:
+    """metrics(result) (propagation.jl:239-242)."""
+    if not _integrity(result):
+        raise P.ArgumentError("propagation result was mutated")
+    return _propagation_metrics(result)
+
+
+def verify(result: PropagationResult, *, temporal_edge_limit=1e-3, spectral_edge_limit=1e-3,
+           min_launch_samples_per_fwhm=8.0, require_launch_sampling=False,
+           photon_drift_limit=1e-4, energy_drift_limit=None) -> dict:
+    """verify(result; ...) (propagation.jl:244-304); None stands for the
+    reference's `missing`."""
+    if not (np.isfinite(temporal_edge_limit) and 0 <= temporal_edge_limit <= 1):
+        raise P.ArgumentError("temporal_edge_limit must be finite and lie in [0, 1]")
+    if not (np.isfinite(spectral_edge_limit) and 0 <= spectral_edge_limit <= 1):
+        raise P.ArgumentError("spectral_edge_limit must be finite and lie in [0, 1]")
+    if not (np.isfinite(min_launch_samples_per_fwhm) and min_launch_samples_per_fwhm > 0):
+        raise P.ArgumentError("min_launch_samples_per_fwhm must be positive and finite")
+    if photon_drift_limit is not None and not (np.isfinite(photon_drift_limit) and
+                                               photon_drift_limit >= 0):
+        raise P.ArgumentError("photon_drift_limit must be nonnegative and finite")
+    if energy_drift_limit is not None and not (np.isfinite(energy_drift_limit) and
+                                               energy_drift_limit >= 0):
+        raise P.ArgumentError("energy_drift_limit must be nonnegative and finite")
+    keys = ("pass", "integrity_ok", "solver_success", "finite_fields",
+            "temporal_edges_contained", "spectral_edges_contained", "launch_sampling_ok",
+            "photon_number_conserved", "energy_change_acceptable", "max_temporal_edge_fraction",
+            "max_spectral_edge_fraction", "launch_samples_per_fwhm", "max_photon_number_drift",
+            "max_relative_energy_change")
+    if not _integrity(result):
+        out = dict.fromkeys(keys)
+        out.update({"pass": False, "integrity_ok": False})
+        return out
+    ev = _propagation_metrics(result)
+    finite = bool(np.all(np.isfinite(result.spectra)))
+    temporal_ok = ev["max_temporal_edge_fraction"] <= temporal_edge_limit
+    spectral_ok = ev["max_spectral_edge_fraction"] <= spectral_edge_limit
+    launch = ev["launch_samples_per_fwhm"]
+    sampling_ok = None if launch is None else launch >= min_launch_samples_per_fwhm
+    sampling_gate = sampling_ok is not False and (not require_launch_sampling or
+                                                  sampling_ok is True)
+    photon_ok = None if photon_drift_limit is None else \
+        ev["max_photon_number_drift"] <= photon_drift_limit
+    energy_ok = None if energy_drift_limit is None else \
+        ev["max_relative_energy_change"] <= energy_drift_limit
+    passed = (finite and temporal_ok and spectral_ok and sampling_gate and
+              photon_ok is not False and energy_ok is not False)
+    return {"pass": bool(passed), "integrity_ok": True, "solver_success": True,
+            "finite_fields": finite, "temporal_edges_contained": bool(temporal_ok),
+            "spectral_edges_contained": bool(spectral_ok), "launch_sampling_ok": sampling_ok,
+            "photon_number_conserved": photon_ok, "energy_change_acceptable": energy_ok,
+            "max_temporal_edge_fraction": ev["max_temporal_edge_fraction"],
+            "max_spectral_edge_fraction": ev["max_spectral_edge_fraction"],
+            "launch_samples_per_fwhm": launch,
+            "max_photon_number_drift": ev["max_photon_number_drift"],
+            "max_relative_energy_change": ev["max_relative_energy_change"]}
 
 
 def phase_gradient(fp: P.FiberProblem, phases, *, log_cost=False, precision="fp32",

@@ -308,3 +308,27 @@ def test_physical_gradient_objectives(gpu_ctx, objective):
     go = (2 * np.real(np.conj(lam0) * 1j * shaped)).sum(axis=0)
     assert abs(J - Jo) <= 1e-4 * abs(Jo)
     assert rel(g["phase"], go) < GRAD_TOL
+
+
+def test_propagate_metrics_and_verify(gpu_ctx):
+    # propagate(problem; saveat) on the GPU, then metrics/verify evidence
+    # (propagation.jl:176-304) on the test_propagation.jl:19-111 shape; the
+    # evidence matches the same reductions over the oracle's spectra
+    from fiberlab_gpu import solve as S
+    fp = P.single_mode_problem(nt=128, time_window_ps=3.0, L=1e-4, power_w=1e-5,
+                               fwhm_s=250e-15, rep_rate_hz=50e6, pulse="gauss",
+                               betas=(-2.17e-26,), beta_order=2)
+    zs = [0.0, 0.5e-4, 1e-4]
+    ref, _, _ = O.forward(fp, zsave=zs)
+    for precision, drift in (("fp64", 1e-8), ("fp32", 1e-5)):
+        res = S.propagate(fp, zs, precision=precision, ctx=gpu_ctx)
+        ev = S.metrics(res)
+        assert ev["max_photon_number_drift"] < drift
+        assert ev["input_energy_pj"] == pytest.approx(0.2, rel=1e-5)
+        for i in range(len(zs)):
+            m, mo = S.field_metrics(res.spectra[i], fp.sim), S.field_metrics(ref[i], fp.sim)
+            assert m["energy_pj"] == pytest.approx(mo["energy_pj"], rel=1e-6)
+            assert m["peak_power_w"] == pytest.approx(mo["peak_power_w"], rel=1e-5)
+        v = S.verify(res)
+        assert v["pass"] and v["integrity_ok"] and v["launch_sampling_ok"]
+        assert not S.verify(res, min_launch_samples_per_fwhm=16)["pass"]
