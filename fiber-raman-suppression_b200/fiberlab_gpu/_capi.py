@@ -147,6 +147,7 @@ class Context:
         if rc:
             raise FiberLabGPUError(rc, lib.fl_status_string(rc).decode())
         self.h = h
+        self.device = int(device)
 
     def check(self, rc: int):
         if rc != FL_OK:

@@ -332,3 +332,28 @@ def test_propagate_metrics_and_verify(gpu_ctx):
         v = S.verify(res)
         assert v["pass"] and v["integrity_ok"] and v["launch_sampling_ok"]
         assert not S.verify(res, min_launch_samples_per_fwhm=16)["pass"]
+
+
+def test_lbfgs_batched_inverse_design(gpu_ctx):
+    # optimize_spectral_phase (raman_optimization.jl:183-246) for two starts
+    # in lockstep: every line search is one batched forward + adjoint launch
+    # over 2 x 4 trial phases; the dB objective with the GDD regulariser
+    import torch
+    from fiberlab_gpu import optimize as OP
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6, raman_threshold_thz=-5.0)
+    gp = GPUProblem(gpu_ctx, fp)
+    obj = OP.BandPhaseObjective(gp, log_cost=True, lambda_gdd=1e-4)
+    x0 = 0.5 * np.random.default_rng(4).standard_normal((2, fp.nt))
+    J0, g0 = obj(torch.from_numpy(x0).to(obj.device))
+    Jb, gb, _ = gp.phase_gradient_batch(x0)
+    Jr, gr = OP.gdd_penalty(torch.from_numpy(x0), fp.sim["Δt"], 1e-4)
+    Jl = torch.from_numpy(Jb) + Jr
+    assert np.allclose(J0.cpu().numpy(), 10 * np.log10(Jl.numpy()), rtol=0, atol=1e-9)
+    ref_g = (torch.from_numpy(gb) + gr) * (10 / (np.log(10) * Jl))[:, None]
+    assert rel(g0.cpu().numpy(), ref_g.numpy()) < 1e-12
+    res = OP.optimize_spectral_phase(gp, x0, max_iter=6, lambda_gdd=1e-4, probes=4)
+    tr = torch.stack([J0.cpu()] + [t.cpu() for t in res.trace])
+    assert torch.all(tr[1:] <= tr[:-1] + 1e-12)
+    assert torch.all(res.J.cpu() < J0.cpu() - 0.1)
+    assert res.iterations.min() >= 1 and res.solves >= 2 * 4 * res.iterations.max()
