@@ -216,3 +216,15 @@ def test_mm_config4_gradient_central_differences(gpu_ctx):
         h = 1e-4
         fd = (cost(ph + h * d) - cost(ph - h * d)) / (2 * h)
         assert abs(fd - np.sum(g[0] * d)) <= GRAD_TOL * abs(fd)
+
+
+def test_mm_grin_fiber_forward(gpu_ctx):
+    # a 3-mode parabolic GRIN fiber from the host mode solver
+    # (fibers.jl:91-132) through the multimode GPU stepper against the oracle
+    from fiberlab_gpu import grin as G
+    fp = G.grin_problem(3, 512, 5.0, 0.3, 4e-9, 200e-15, nx=48, weights=[0.8, 0.5, 0.33],
+                        raman_threshold_thz=-5.0)
+    out, st = GPUProblem(gpu_ctx, fp).forward()
+    ref, _, _ = O.forward(fp)
+    assert st["status"] == 0
+    assert rel(out[-1], ref[-1]) < FIELD_TOL_FP32
