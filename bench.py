@@ -241,6 +241,40 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3, window_s=0.0):
     return out
 
 
+def optimizer_measure(ctx, B, probes, iters):
+    """The inverse-design consumer of the batched gradient: B independent
+    L-BFGS optimisations of the headline problem's phase (dB band objective
+    with the reference's default GDD weight 1e-4), each line search one
+    batched forward + adjoint launch over B x probes trial phases.  Reports
+    accepted iterations per second over all B problems, the cost/gradient
+    evaluations per second behind them, and the median improvement."""
+    import torch
+    from fiberlab_gpu import optimize as OP
+    from fiberlab_gpu._capi import GPUProblem
+    fp = workload_problem()
+    gp = GPUProblem(ctx, fp)
+    x0 = phases(77, B, fp.nt)
+    obj = OP.BandPhaseObjective(gp, log_cost=True, lambda_gdd=1e-4)
+    # warm-up at the line-search batch size (workspace allocation outside the timing)
+    obj(torch.from_numpy(np.repeat(x0, probes, axis=0)).to(obj.device))
+    solves0 = obj.solves
+    J0, _ = obj(torch.from_numpy(x0).to(obj.device))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = OP.lbfgs(obj, torch.from_numpy(x0).to(obj.device), max_iter=iters, f_abstol=None,
+                   probes=probes)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    gain = (J0 - res.J).cpu().numpy()
+    return {"workload": f"{B} L-BFGS optimisations of the headline problem (dB band + GDD 1e-4),"
+                        f" {probes} trial steps per line search, {iters} iterations",
+            "iterations_per_s": float(res.iterations.sum()) / dt,
+            "solves_per_s": (obj.solves - solves0 - B) / dt,
+            "ms_per_iteration": 1e3 * dt / max(1, int(res.iterations.max())),
+            "median_db_improvement": float(np.median(gain)),
+            "line_search_launches": int(res.evaluations - 1)}
+
+
 def multimode_measure(ctx, dev, B, steps, warmup):
     """Config 4: B per-mode phase candidates φ ~ N(0, 1) (seeded) of the M = 10
     HG(m+n<=3) problem on a 96x96 grid, Nt = 2^14 over 10 ps, L = 2 m, 5 nJ,
@@ -446,6 +480,10 @@ def run_ours(args):
     if args.mm_batch and rank == 0 and world == 1:
         multimode = multimode_measure(ctx, dev, args.mm_batch, min(args.steps, 3), 1)
 
+    optimizer = None
+    if args.opt_batch and rank == 0 and world == 1:
+        optimizer = optimizer_measure(ctx, args.opt_batch, args.opt_probes, args.opt_iters)
+
     serving = None
     if args.serve and rank == 0:
         serving = serving_measure(Context, local, args.serve, args.serve_plain,
@@ -469,6 +507,8 @@ def run_ours(args):
                 "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B}}
         if multimode is not None:
             line.update(multimode)
+        if optimizer is not None:
+            line["inverse_design"] = optimizer
         if serving is not None:
             line["serving"] = serving
         print(json.dumps(line), flush=True)
@@ -487,6 +527,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mm-batch", type=int, default=64,
                     help="config-4 candidates per batch reported beside the headline (0: off)")
+    ap.add_argument("--opt-batch", type=int, default=148,
+                    help="L-BFGS optimisations run in lockstep beside the headline (0: off)")
+    ap.add_argument("--opt-probes", type=int, default=4, help="trial steps per line search")
+    ap.add_argument("--opt-iters", type=int, default=3, help="L-BFGS iterations timed")
     ap.add_argument("--serve", type=int, default=0,
                     help="also run the config-3 serving stream with this many requests")
     ap.add_argument("--serve-window", type=float, default=0.0,
