@@ -137,6 +137,8 @@ struct fl_problem {
     int nt = 0, m = 0, precision = 0;
     double one_m_fR = 0, L = 0, reltol = 0, abstol = 0, gamma0 = 0;
     bool gamma_sym = true;
+    int objective = OBJ_RAMAN_BAND;        // terminal objective of the gradient entry points
+    double obj_tau = 50.0;                 // worst-mode smoothness
     bool use_mm = false;  // multimode runtime: M > 1, or M = 1 beyond one CTA's transform (2^15)
     double* d_Dturns = nullptr;
     void* d_Heff[2] = {nullptr, nullptr};  // [0] float, [1] double
@@ -396,12 +398,16 @@ int new_work(fl_problem* pr, int B, int nsave, int mode, Work** w) {
     return work_create(pr, B, nsave, mode, w);
 }
 
-// rewrite the mode of every descriptor (host image + device copy)
-int set_mode(fl_ctx* ctx, Work* w, int mode, int log_cost) {
+// rewrite the mode (and the objective of a gradient mode) of every
+// descriptor (host image + device copy)
+int set_mode(fl_ctx* ctx, Work* w, int mode, int log_cost, int objective = OBJ_RAMAN_BAND,
+             double tau = 50.0) {
     for (int b = 0; b < w->B; b++) {
         SlotDesc* d = reinterpret_cast<SlotDesc*>(w->h_desc.data()) + b;
         d->mode = mode;
         d->log_cost = log_cost;
+        d->objective = objective;
+        d->obj_tau = tau;
     }
     CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), w->h_desc.size(), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -572,10 +578,13 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     return FL_OK;
 }
 
-int mm_set_mode(fl_ctx* ctx, MmWork* w, int mode, int log_cost) {
+int mm_set_mode(fl_ctx* ctx, MmWork* w, int mode, int log_cost, int objective = OBJ_RAMAN_BAND,
+                double tau = 50.0) {
     for (auto& d : w->h_desc) {
         d.mode = mode;
         d.log_cost = log_cost;
+        d.objective = objective;
+        d.obj_tau = tau;
     }
     CU(cudaMemcpyAsync(w->d_desc, w->h_desc.data(), sizeof(MmDesc) * w->B, cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -820,7 +829,7 @@ int mm_phase_gradient_device(fl_problem* pr, const double* d_u0, int nbatch,
     }
     MmWork* w = pr->mlast;
     CU(cudaEventRecord(ctx->ev[0], ctx->stream));
-    int rc = mm_set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost);
+    int rc = mm_set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost, pr->objective, pr->obj_tau);
     if (rc) return rc;
     CU(cudaMemsetAsync(w->d_state, 0, sizeof(MmState) * nbatch, ctx->stream));
     CU(cudaMemcpyAsync(w->d_mask, d_mask, nt, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -872,6 +881,8 @@ struct SrvRequest {
     int weight = 1;                    // CTAs per transform of its slot
     fl_problem* prob = nullptr;
     int kind = FL_REQ_FORWARD, log_cost = 0;
+    int objective = OBJ_RAMAN_BAND;    // the problem's objective when submitted
+    double obj_tau = 50.0;
     double L = 0;
     std::vector<double> u0;            // shaped launch, (Nt, M) complex
     std::vector<unsigned char> mask;
@@ -1041,6 +1052,8 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
         d.abstol = pr->abstol;
         d.mode = mode;
         d.log_cost = r->log_cost;
+        d.objective = r->objective;
+        d.obj_tau = r->obj_tau;
         d.phase_per_mode = 0;
         d.mask = dmask;
         // a forward-only request keeps no checkpoints or step log
@@ -1064,6 +1077,8 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
         d.abstol = pr->abstol;
         d.mode = mode;
         d.log_cost = r->log_cost;
+        d.objective = r->objective;
+        d.obj_tau = r->obj_tau;
         d.mask = dmask;
         // a forward-only request keeps no checkpoints or step log
         d.ck_cap = mode == MODE_FORWARD ? 0 : c->w->K;
@@ -1436,6 +1451,18 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
     return FL_OK;
 }
 
+int fl_problem_set_objective(fl_problem* pr, int objective, double worst_mode_tau) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    if (objective < FL_OBJ_RAMAN_BAND || objective > FL_OBJ_RAMAN_PEAK)
+        return set_err(pr->ctx, FL_EINVAL, "unknown objective %d", objective);
+    if (!(std::isfinite(worst_mode_tau) && worst_mode_tau > 0))
+        return set_err(pr->ctx, FL_EINVAL, "worst-mode smoothness tau must be positive and finite");
+    pr->objective = objective;
+    pr->obj_tau = worst_mode_tau;
+    return FL_OK;
+}
+
 int fl_problem_destroy(fl_problem* pr) {
     if (!pr) return FL_EINVAL;
     delete pr->last;
@@ -1579,7 +1606,7 @@ static int phase_gradient_core(fl_problem* pr, Work* w, int nbatch, const double
     fl_ctx* ctx = pr->ctx;
     const int nt = pr->nt;
     CU(cudaEventRecord(ctx->ev[0], ctx->stream));
-    int rc = set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost);
+    int rc = set_mode(ctx, w, MODE_BAND_GRADIENT, log_cost, pr->objective, pr->obj_tau);
     if (rc) return rc;
     CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState) * nbatch, ctx->stream));
     CU(cudaMemcpyAsync(w->d_mask, d_mask, nt, cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1800,6 +1827,8 @@ int fl_server_submit(fl_server* sv, const fl_request* q, long* id) {
     r->weight = pr->use_mm ? pr->m * mm_cluster_ctas(logn) : 1;
     r->kind = q->kind;
     r->log_cost = q->log_cost;
+    r->objective = pr->objective;
+    r->obj_tau = pr->obj_tau;
     r->L = L;
     const size_t nm = (size_t)pr->nt * pr->m;
     r->u0.assign(q->u0, q->u0 + 2 * nm);

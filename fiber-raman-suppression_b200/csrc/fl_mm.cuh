@@ -657,6 +657,7 @@ __global__ void __launch_bounds__(kMmTB)
 // integrator to its next evaluation (one CTA per slot, block-uniform state)
 // ---------------------------------------------------------------------------
 constexpr int kMmCtl = 512;
+constexpr int kMmMaxModes = 10;  // modes of the built multimode shapes
 
 struct MmCtl {
     const MmDesc& d;
@@ -1036,24 +1037,94 @@ struct MmCtl {
         const double* uf = d.u[st.cur];
         double* lam = d.lam[0];
         if (d.mode == MODE_BAND_GRADIENT) {
-            double et = 0.0, eb = 0.0;
-            for (size_t i = threadIdx.x; i < NM; i += kMmCtl) {
-                const cx<double> x = ld2(uf, i);
-                const double e = x.re * x.re + x.im * x.im;
-                et += e;
-                if (d.mask[i % N]) eb += e;
+            // The objectives of physics_helpers.jl:222-302.  Each seed is
+            // u(L) times a real factor per (mode, bin) -- a_m (sel - r_m) --
+            // so the interaction-frame seed is ũ(L) times the same factor:
+            //   band         a = 1/E,          r = J, sel = band mask
+            //   fundamental  a_0 = 1/E_0, 0 on the other modes, r = J
+            //   worst mode   a_m = w_m/E_m (w = softmax τ r over the modes
+            //                with energy), r_m = mode m's band fraction
+            //   peak         a = 1/E, r = J, sel = the strongest in-band bin
+            //                (mode-summed energy, lowest index among equals)
+            const int M = d.M, obj = d.objective;
+            double a[kMmMaxModes], r[kMmMaxModes];
+            double cost;
+            int pk = -1;
+            if (obj == OBJ_FUNDAMENTAL || obj == OBJ_WORST_MODE) {
+                double tm[kMmMaxModes];
+                for (int m = 0; m < M; m++) {
+                    double et = 0.0, eb = 0.0;
+                    for (int t = threadIdx.x; t < N; t += kMmCtl) {
+                        const double e = energy(ld2(uf, (size_t)m * N + t));
+                        et += e;
+                        if (d.mask[t]) eb += e;
+                    }
+                    tm[m] = sum(et);
+                    const double bm = sum(eb);
+                    r[m] = tm[m] > 0.0 ? bm / tm[m] : 0.0;
+                    a[m] = 0.0;
+                }
+                if (obj == OBJ_FUNDAMENTAL) {
+                    cost = r[0];
+                    a[0] = 1.0 / tm[0];
+                    for (int m = 1; m < M; m++) r[m] = 0.0;
+                } else {
+                    double rmax = -1.0;
+                    int K = 0;
+                    for (int m = 0; m < M; m++)
+                        if (tm[m] > 0.0) {
+                            rmax = fmax(rmax, r[m]);
+                            K++;
+                        }
+                    double den = 0.0;
+                    for (int m = 0; m < M; m++)
+                        if (tm[m] > 0.0) den += exp(d.obj_tau * (r[m] - rmax));
+                    cost = rmax + (log(den) - log((double)K)) / d.obj_tau;
+                    for (int m = 0; m < M; m++)
+                        a[m] = tm[m] > 0.0 ? exp(d.obj_tau * (r[m] - rmax)) / den / tm[m] : 0.0;
+                }
+            } else {
+                double et = 0.0, eb = 0.0, emax = -1.0;
+                for (int t = threadIdx.x; t < N; t += kMmCtl) {
+                    double e = 0.0;
+                    for (int m = 0; m < M; m++) e += energy(ld2(uf, (size_t)m * N + t));
+                    et += e;
+                    if (d.mask[t]) {
+                        eb += e;
+                        emax = fmax(emax, e);
+                    }
+                }
+                const double tot = sum(et);
+                double band = sum(eb);
+                if (obj == OBJ_RAMAN_PEAK) {
+                    band = maxv(emax);
+                    // lowest index as the largest key N - t (maxv folds from 0)
+                    double key = 0.0;
+                    for (int t = threadIdx.x; t < N; t += kMmCtl) {
+                        double e = 0.0;
+                        for (int m = 0; m < M; m++) e += energy(ld2(uf, (size_t)m * N + t));
+                        if (d.mask[t] && e == band) key = fmax(key, (double)(N - t));
+                    }
+                    pk = N - (int)maxv(key);
+                }
+                cost = band / tot;
+                for (int m = 0; m < M; m++) {
+                    a[m] = 1.0 / tot;
+                    r[m] = cost;
+                }
             }
-            const double tot = sum(et), band = sum(eb);
-            const double cost = band / tot;
-            double sc = 1.0 / tot;
+            double sc = 1.0;
             st.J = cost;
             if (d.log_cost) {  // physics_helpers.jl:320-326
                 st.J = 10.0 * log10(fmax(cost, 1e-15));
-                sc *= cost <= 1e-15 ? 0.0 : 10.0 / (log(10.0) * cost);
+                sc = cost <= 1e-15 ? 0.0 : 10.0 / (log(10.0) * cost);
             }
             for (size_t i = threadIdx.x; i < NM; i += kMmCtl) {
+                const int m = (int)(i / N), t = (int)(i % N);
                 const cx<double> x = ld2(uf, i);
-                const double f = ((d.mask[i % N] ? 1.0 : 0.0) - cost) * sc;
+                const double sel = obj == OBJ_RAMAN_PEAK ? (t == pk ? 1.0 : 0.0)
+                                                         : (d.mask[t] ? 1.0 : 0.0);
+                const double f = a[m] * (sel - r[m]) * sc;
                 st2(lam, i, mk(x.re * f, x.im * f));
             }
         } else {

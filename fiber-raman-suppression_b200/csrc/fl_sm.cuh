@@ -94,6 +94,11 @@ __device__ __forceinline__ cx<double> ld2(const double* p, int b) {
 __device__ __forceinline__ void st2(double* p, int b, cx<double> v) {
     reinterpret_cast<double2*>(p)[b] = make_double2(v.re, v.im);
 }
+// |x|² rounded the same way wherever it is evaluated (no contraction choice
+// left to the compiler), so energies of one field compare exactly
+__device__ __forceinline__ double energy(cx<double> x) {
+    return __fma_rn(x.re, x.re, __dmul_rn(x.im, x.im));
+}
 template <typename R>
 __device__ __forceinline__ cx<double> up(cx<R> a) {
     return mk((double)a.re, (double)a.im);
@@ -660,17 +665,37 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double* uf = d.u[st.cur];
             double* lam = d.lam[0];
             if (d.mode == MODE_BAND_GRADIENT) {
-                double et = 0.0, eb = 0.0;
+                // Band objective (physics_helpers.jl:222-232).  With one mode
+                // the fundamental-mode and worst-mode objectives are the same
+                // (:234-286: one active mode, log-sum-exp = its fraction,
+                // weight 1).  The peak objective (:288-302) puts the strongest
+                // in-band bin (lowest index among equals) in place of the band.
+                const bool peak = d.objective == OBJ_RAMAN_PEAK;
+                double et = 0.0, eb = 0.0, emax = -1.0;
 #pragma unroll
                 for (int s = 0; s < E; s++) {
                     const int b = SolF::bin(s);
-                    const cx<double> x = ld2(uf, b);
-                    const double e = x.re * x.re + x.im * x.im;
+                    const double e = energy(ld2(uf, b));
                     et += e;
-                    if (d.mask[b]) eb += e;
+                    if (d.mask[b]) {
+                        eb += e;
+                        emax = fmax(emax, e);
+                    }
                 }
                 const double tot = block_sum<T>(et, red);
-                const double band = block_sum<T>(eb, red);
+                double band = block_sum<T>(eb, red);
+                int pk = -1;
+                if (peak) {
+                    band = block_max<T>(emax, red);
+                    // lowest index as the largest key N - b (block_max folds from 0)
+                    double key = 0.0;
+#pragma unroll
+                    for (int s = 0; s < E; s++) {
+                        const int b = SolF::bin(s);
+                        if (d.mask[b] && energy(ld2(uf, b)) == band) key = fmax(key, (double)(N - b));
+                    }
+                    pk = N - (int)block_max<T>(key, red);
+                }
                 const double cost = band / tot;
                 double sc = 1.0 / tot;
                 st.J = cost;
@@ -678,12 +703,13 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     st.J = 10.0 * log10(fmax(cost, 1e-15));
                     sc *= cost <= 1e-15 ? 0.0 : 10.0 / (log(10.0) * cost);
                 }
-                // e^{-iDL} (u_L (mask - J)/E) = ũ(L) (mask - J)/E
+                // e^{-iDL} (u_L (sel - J)/E) = ũ(L) (sel - J)/E, sel the band or peak bin
 #pragma unroll
                 for (int s = 0; s < E; s++) {
                     const int b = SolF::bin(s);
                     const cx<double> x = ld2(uf, b);
-                    const double f = ((d.mask[b] ? 1.0 : 0.0) - cost) * sc;
+                    const double sel = peak ? (b == pk ? 1.0 : 0.0) : (d.mask[b] ? 1.0 : 0.0);
+                    const double f = (sel - cost) * sc;
                     st2(lam, b, mk(x.re * f, x.im * f));
                 }
             } else {

@@ -11,6 +11,15 @@ enum SlotMode : int {
     MODE_SEEDED_ADJOINT = 2  // forward + adjoint from a caller-supplied terminal seed
 };
 
+// Terminal objective of MODE_BAND_GRADIENT (its cost and adjoint seed);
+// the values of FL_OBJ_* in the C-ABI header.
+enum SlotObjective : int {
+    OBJ_RAMAN_BAND = 0,   // mode-summed band fraction
+    OBJ_FUNDAMENTAL = 1,  // band fraction of mode 1
+    OBJ_WORST_MODE = 2,   // log-sum-exp of the per-mode band fractions
+    OBJ_RAMAN_PEAK = 3    // strongest in-band bin (summed over modes) over the total
+};
+
 enum SlotPhase : int {
     PH_FWD_INIT = 0,
     PH_FWD = 1,
@@ -46,6 +55,8 @@ struct SlotDesc {
     double gamma, one_m_fR;
     double L, reltol, abstol;
     int mode, log_cost;
+    int objective;          // SlotObjective of MODE_BAND_GRADIENT
+    double obj_tau;         // worst-mode smoothness τ
     int nsave;
     int ck_cap;             // checkpoint slots K (power of two)
     int seg_cap;            // steps per recompute segment buffer
@@ -118,6 +129,8 @@ struct MmDesc {
     double one_m_fR;
     double L, reltol, abstol;
     int mode, log_cost, nsave;
+    int objective;          // SlotObjective of MODE_BAND_GRADIENT
+    double obj_tau;         // worst-mode smoothness τ
     int phase_per_mode;     // gradient: 1 = one phase per (t, m); 0 = phase shared by the modes
     int ck_cap, seg_cap, step_cap;
     long max_iters;

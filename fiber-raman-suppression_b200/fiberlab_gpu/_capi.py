@@ -27,7 +27,13 @@ EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_phase_gradient_batch_device", "fl_rhs_eval", "fl_ctx_timing",
            "fl_forward_noalloc", "fl_mode_phase_gradient_batch",
            "fl_mode_phase_gradient_batch_device", "fl_server_create", "fl_server_destroy",
-           "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_info_get")
+           "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_info_get",
+           "fl_problem_set_objective")
+
+# device objectives (FL_OBJ_*) by the reference's objective names
+# (physics_models.jl:947-962); temporal_width runs with a host seed
+OBJECTIVE = {"raman_band": 0, "mode_sum": 0, "mmf_sum": 0, "fundamental_mode": 1,
+             "mmf_fundamental": 1, "worst_mode": 2, "mmf_worst_mode": 2, "raman_peak": 3}
 
 
 class FlCtxOpts(C.Structure):
@@ -97,6 +103,7 @@ def load() -> C.CDLL:
         lib.fl_problem_create.argtypes = [vp, ip, ip, vp, vp, vp, vp, dp, dp, dp, dp, ip,
                                           C.POINTER(vp)]
         lib.fl_problem_destroy.argtypes = [vp]
+        lib.fl_problem_set_objective.argtypes = [vp, ip, dp]
         lib.fl_forward.argtypes = [vp, vp, vp, ip, vp, C.POINTER(FlStats)]
         lib.fl_adjoint.argtypes = [vp, vp, vp, C.POINTER(FlStats)]
         lib.fl_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
@@ -194,6 +201,17 @@ class GPUProblem:
                                            float(fp.L), float(fp.reltol), float(fp.abstol),
                                            PRECISION[precision], C.byref(h)))
         self.h = h
+        self.objective = "raman_band"
+
+    def set_objective(self, name: str, worst_mode_tau: float = 50.0):
+        """Objective of the batched gradient calls and band-gradient server
+        requests of this problem (fl_problem_set_objective)."""
+        if name not in OBJECTIVE:
+            raise ValueError(f"objective {name!r} has no device seed; device objectives: "
+                             f"{', '.join(sorted(OBJECTIVE))}")
+        self.ctx.check(load().fl_problem_set_objective(self.h, OBJECTIVE[name],
+                                                       float(worst_mode_tau)))
+        self.objective = name
 
     def forward(self, u0=None, saveat=None):
         fp = self.fp

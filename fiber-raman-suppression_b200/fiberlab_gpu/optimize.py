@@ -103,13 +103,16 @@ def apply_log_surface(J: torch.Tensor, grad: torch.Tensor):
 
 
 class BandPhaseObjective:
-    """Regularised Raman-band objective of one problem for a batch of shared
+    """Regularised field objective of one problem for a batch of shared
     phases: phis (K, Nt) float64 on the device -> J (K,), ∂J/∂φ (K, Nt), with
     every forward + adjoint of the K phases in one batched launch
-    (cost_and_gradient, raman_optimization.jl:102-177)."""
+    (cost_and_gradient, raman_optimization.jl:102-177).  The objective is the
+    Raman band by default, or any objective with a device seed
+    (GPUProblem.set_objective: fundamental_mode, worst_mode, raman_peak)."""
 
     def __init__(self, gp: GPUProblem, *, log_cost: bool = True, lambda_gdd: float = 0.0,
-                 lambda_boundary: float = 0.0, device=None):
+                 lambda_boundary: float = 0.0, device=None, objective: str = "raman_band",
+                 worst_mode_tau: float = 50.0):
         fp = gp.fp
         if fp.mask is None or not np.any(fp.mask):
             raise P.ArgumentError("band mask must contain at least one bin")
@@ -117,6 +120,7 @@ class BandPhaseObjective:
             if not (math.isfinite(v) and v >= 0):
                 raise P.ArgumentError(f"regularizer `{name}` lambda must be nonnegative and finite")
         self.gp, self.fp = gp, fp
+        gp.set_objective(objective, worst_mode_tau)
         self.log_cost = log_cost
         self.lambda_gdd, self.lambda_boundary = float(lambda_gdd), float(lambda_boundary)
         self.device = torch.device(device or f"cuda:{gp.ctx.device}")

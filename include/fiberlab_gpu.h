@@ -108,6 +108,23 @@ int fl_problem_create(fl_ctx *ctx, int nt, int m, const double *D, const double 
                       double reltol, double abstol, int precision, fl_problem **out);
 int fl_problem_destroy(fl_problem *prob);
 
+/* Terminal objective of the batched gradient entry points
+ * (fl_phase_gradient_batch*, fl_mode_phase_gradient_batch*) and of the
+ * problem's band-gradient server requests, computed on the device with its
+ * seed λ(L) = ∂J/∂conj(u(L)).  Replaces the choice among the reference's
+ * objective constructors raman_band_objective / fundamental_mode_objective /
+ * worst_mode_objective / raman_peak_objective (physics_models.jl:851-932),
+ * whose costs are physics_helpers.jl:222-302.  (temporal_width needs a
+ * transform of the output; run it with fl_forward + fl_adjoint and a host
+ * seed.)  The default is FL_OBJ_RAMAN_BAND; worst_mode_tau is the
+ * log-sum-exp smoothness τ (reference default 50).  For M = 1 the
+ * fundamental-mode and worst-mode objectives equal the band objective. */
+#define FL_OBJ_RAMAN_BAND 0  /* mode-summed band fraction */
+#define FL_OBJ_FUNDAMENTAL 1 /* band fraction of mode 1; seed zero on the others */
+#define FL_OBJ_WORST_MODE 2  /* normalised log-sum-exp of the per-mode band fractions */
+#define FL_OBJ_RAMAN_PEAK 3  /* strongest in-band bin (summed over modes) over the total */
+int fl_problem_set_objective(fl_problem *prob, int objective, double worst_mode_tau);
+
 /* Forward solve 0 -> L.  Replaces solve_disp_mmf (simulate_disp_mmf.jl:183-207)
  * as used by propagate (propagation.jl:89-123): out_spectra receives the
  * lab-frame spectra cis(D z) ũ(z) at each saveat position (Nt*M*nsave

@@ -228,3 +228,26 @@ def test_mm_grin_fiber_forward(gpu_ctx):
     ref, _, _ = O.forward(fp)
     assert st["status"] == 0
     assert rel(out[-1], ref[-1]) < FIELD_TOL_FP32
+
+
+@pytest.mark.parametrize("objective", ["fundamental_mode", "worst_mode", "raman_peak"])
+@pytest.mark.parametrize("log_cost", [False, True])
+def test_mm_device_objective_seeds(gpu_ctx, objective, log_cost):
+    # multimode device seeds (fl_problem_set_objective) against the oracle's
+    # forward and adjoint with the host seed of the same objective
+    from fiberlab_gpu import objectives as Ob
+    fp = hg_problem(3, 512, L=0.5, energy=6e-9)
+    phi = 0.5 * np.random.default_rng(12).standard_normal(fp.nt)
+    gp = GPUProblem(gpu_ctx, fp)
+    gp.set_objective(objective, 20.0)
+    J, g, _ = gp.phase_gradient_batch(phi[None, :], log_cost=log_cost)
+    shaped = fp.uw0 * np.exp(1j * phi)[None, :]
+    out, _, dense = O.forward(fp, u0=shaped, keep_dense=True)
+    Jo, seed = Ob.cost_and_seed(objective, out[-1], fp.mask, fp.sim, log_cost, worst_mode_tau=20.0)
+    lam0, _ = O.adjoint(fp, dense, seed)
+    go = (2 * np.real(np.conj(lam0) * 1j * shaped)).sum(axis=0)
+    if log_cost:
+        assert abs(J[0] - Jo) < DB_TOL
+    else:
+        assert abs(J[0] - Jo) <= 1e-4 * abs(Jo)
+    assert rel(g[0], go) < GRAD_TOL

@@ -357,3 +357,30 @@ def test_lbfgs_batched_inverse_design(gpu_ctx):
     assert torch.all(tr[1:] <= tr[:-1] + 1e-12)
     assert torch.all(res.J.cpu() < J0.cpu() - 0.1)
     assert res.iterations.min() >= 1 and res.solves >= 2 * 4 * res.iterations.max()
+
+
+@pytest.mark.parametrize("objective", ["fundamental_mode", "worst_mode", "raman_peak"])
+def test_device_objective_seeds_single_mode(gpu_ctx, objective):
+    # fl_problem_set_objective: the batched call computes J and the seed on
+    # the device; against the oracle's forward and adjoint with the host seed
+    from fiberlab_gpu import objectives as Ob
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6, raman_threshold_thz=-5.0)
+    phi = 0.5 * np.random.default_rng(8).standard_normal(fp.nt)
+    gp = GPUProblem(gpu_ctx, fp)
+    Jband, _, _ = gp.phase_gradient_batch(phi[None, :])
+    gp.set_objective(objective)
+    J, g, _ = gp.phase_gradient_batch(phi[None, :])
+    shaped = fp.uw0 * np.exp(1j * phi)[None, :]
+    out, _, dense = O.forward(fp, u0=shaped, keep_dense=True)
+    Jo, seed = Ob.cost_and_seed(objective, out[-1], fp.mask, fp.sim)
+    lam0, _ = O.adjoint(fp, dense, seed)
+    go = (2 * np.real(np.conj(lam0) * 1j * shaped)).sum(axis=0)
+    assert abs(J[0] - Jo) <= 1e-4 * abs(Jo)
+    assert rel(g[0], go) < GRAD_TOL
+    if objective != "raman_peak":   # one mode: the band objective itself
+        assert J[0] == Jband[0]
+    gp.set_objective("raman_band")
+    assert gp.phase_gradient_batch(phi[None, :])[0][0] == Jband[0]
+    with pytest.raises(ValueError):
+        gp.set_objective("temporal_width")
