@@ -147,6 +147,9 @@ struct fl_problem {
     void* d_G[2] = {nullptr, nullptr};     // multimode contraction matrix [0] float, [1] double
     double* d_Ga = nullptr;                // its adjoint layout
     float* d_Gtc = nullptr;                // its tensor-core operand image (M >= 6)
+    // device staging of the host-buffer batch calls (grow-only, reused)
+    char* d_stage = nullptr;
+    size_t stage_bytes = 0;
     // workspace of the last forward (kept for fl_adjoint)
     struct Work* last = nullptr;
     struct MmWork* mlast = nullptr;        // same for multimode problems
@@ -1467,6 +1470,7 @@ int fl_problem_destroy(fl_problem* pr) {
     if (!pr) return FL_EINVAL;
     delete pr->last;
     delete pr->mlast;
+    cudaFree(pr->d_stage);
     cudaFree(pr->d_G[0]);
     cudaFree(pr->d_G[1]);
     cudaFree(pr->d_Ga);
@@ -1694,13 +1698,28 @@ static int phase_gradient_host(fl_problem* pr, const double* u0, int nbatch,
     for (size_t i = 0; i < np; i++)
         if (!std::isfinite(phases[i])) return set_err(ctx, FL_EINVAL, "phase values must be finite");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
-    double *d_u0 = nullptr, *d_ph = nullptr, *d_J = nullptr, *d_g = nullptr;
-    unsigned char* d_m = nullptr;
-    CU(cudaMallocAsync(&d_u0, 16 * nm, ctx->stream));
-    CU(cudaMallocAsync(&d_ph, 8 * np, ctx->stream));
-    CU(cudaMallocAsync(&d_J, 8 * (size_t)nbatch, ctx->stream));
-    CU(cudaMallocAsync(&d_g, 8 * np, ctx->stream));
-    CU(cudaMallocAsync(&d_m, nt, ctx->stream));
+    // inputs and outputs in the problem's staging area: one allocation that
+    // grows to the largest batch seen and is reused by later calls
+    auto up256 = [](size_t b) { return (b + 255) & ~size_t(255); };
+    const size_t need = up256(16 * nm) + 2 * up256(8 * np) + up256(8 * (size_t)nbatch) + up256(nt);
+    if (need > pr->stage_bytes) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        cudaFree(pr->d_stage);
+        pr->d_stage = nullptr;
+        pr->stage_bytes = 0;
+        CU(cudaMalloc(&pr->d_stage, need));
+        pr->stage_bytes = need;
+    }
+    char* sp = pr->d_stage;
+    double* d_u0 = reinterpret_cast<double*>(sp);
+    sp += up256(16 * nm);
+    double* d_ph = reinterpret_cast<double*>(sp);
+    sp += up256(8 * np);
+    double* d_g = reinterpret_cast<double*>(sp);
+    sp += up256(8 * np);
+    double* d_J = reinterpret_cast<double*>(sp);
+    sp += up256(8 * (size_t)nbatch);
+    unsigned char* d_m = reinterpret_cast<unsigned char*>(sp);
     CU(cudaMemcpyAsync(d_u0, u0, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(d_ph, phases, 8 * np, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(d_m, mask, nt, cudaMemcpyHostToDevice, ctx->stream));
@@ -1709,11 +1728,6 @@ static int phase_gradient_host(fl_problem* pr, const double* u0, int nbatch,
         CU(cudaMemcpyAsync(J, d_J, 8 * (size_t)nbatch, cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(grad, d_g, 8 * np, cudaMemcpyDeviceToHost, ctx->stream));
     }
-    cudaFreeAsync(d_u0, ctx->stream);
-    cudaFreeAsync(d_ph, ctx->stream);
-    cudaFreeAsync(d_J, ctx->stream);
-    cudaFreeAsync(d_g, ctx->stream);
-    cudaFreeAsync(d_m, ctx->stream);
     CU(cudaStreamSynchronize(ctx->stream));
     return rc;
 }
