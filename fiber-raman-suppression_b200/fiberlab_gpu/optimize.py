@@ -108,7 +108,8 @@ class BandPhaseObjective:
     every forward + adjoint of the K phases in one batched launch
     (cost_and_gradient, raman_optimization.jl:102-177).  The objective is the
     Raman band by default, or any objective with a device seed
-    (GPUProblem.set_objective: fundamental_mode, worst_mode, raman_peak)."""
+    (GPUProblem.set_objective: fundamental_mode, worst_mode, raman_peak);
+    constructing it sets that objective on the problem."""
 
     def __init__(self, gp: GPUProblem, *, log_cost: bool = True, lambda_gdd: float = 0.0,
                  lambda_boundary: float = 0.0, device=None, objective: str = "raman_band",

@@ -257,6 +257,13 @@ def test_status_codes_without_a_fault(gpu_ctx):
         GPUProblem(Context(0, checkpoints=2, segment_steps=1), long).phase_gradient_batch(
             np.zeros((1, long.nt)))
     assert e.value.status == 9
+    # objective codes and the worst-mode smoothness are checked at the boundary
+    from fiberlab_gpu._capi import load
+    gp = GPUProblem(gpu_ctx, fp)
+    for code, tau in ((7, 50.0), (-1, 50.0), (2, 0.0), (2, float("nan"))):
+        with pytest.raises(FiberLabGPUError) as e:
+            gp.ctx.check(load().fl_problem_set_objective(gp.h, code, tau))
+        assert e.value.status == 1
 
 
 def test_physical_gradient_phase_amplitude_energy(gpu_ctx):
