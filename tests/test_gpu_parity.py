@@ -391,3 +391,46 @@ def test_device_objective_seeds_single_mode(gpu_ctx, objective):
     assert gp.phase_gradient_batch(phi[None, :])[0][0] == Jband[0]
     with pytest.raises(ValueError):
         gp.set_objective("temporal_width")
+
+
+def test_boundary_rejects_bad_input(gpu_ctx):
+    # the C-ABI's input checks (the reference's ArgumentError cases,
+    # propagation.jl:41-70, physics_helpers.jl:222-232): each call fails with
+    # a status and a message, launches nothing, and the context stays usable
+    fp = P.single_mode_problem(nt=256, time_window_ps=3.0, L=0.3, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    gp = GPUProblem(gpu_ctx, fp)
+
+    def status(fn):
+        with pytest.raises(FiberLabGPUError) as e:
+            fn()
+        return e.value.status
+    # shapes that are not built: Nt beyond 2^15 or below 2^6, more than 10 modes
+    for nt in (65536, 32):
+        big = P.single_mode_problem(nt=nt, time_window_ps=10.0 if nt > 256 else 3.0, L=0.1,
+                                    power_w=0.1, rep_rate_hz=80.5e6, validate_grid=False)
+        assert status(lambda: GPUProblem(gpu_ctx, big)) == 10
+    M = 11
+    many = P.FiberProblem(sim=dict(fp.sim, M=M), D=np.zeros((M, fp.nt)),
+                          gamma=np.full((M, M, M, M), 1e-3), hR=fp.hR, one_m_fR=fp.one_m_fR,
+                          L=fp.L, uw0=np.repeat(fp.uw0, M, axis=0) / np.sqrt(M))
+    assert status(lambda: GPUProblem(gpu_ctx, many)) == 10
+    # an adjoint needs a preceding forward
+    assert status(lambda: gp.adjoint(fp.uw0)) == 1
+    # save positions: sorted, unique, from 0 to L
+    for zs in ([0.0, 0.2, 0.1, fp.L], [0.0, 0.1, 0.1, fp.L], [0.0, 0.1], [0.05, fp.L],
+               [0.0, float("nan"), fp.L]):
+        assert status(lambda: gp.forward(saveat=zs)) == 1
+    # launch spectra: finite and nonzero
+    bad = fp.uw0.copy()
+    bad[0, 3] = np.nan
+    assert status(lambda: gp.forward(bad)) == 1
+    assert status(lambda: gp.forward(np.zeros_like(fp.uw0))) == 1
+    # band objective: a nonempty mask and finite phases
+    phi = np.zeros((2, fp.nt))
+    assert status(lambda: gp.phase_gradient_batch(phi, np.zeros(fp.nt, bool))) == 1
+    phi[1, 7] = np.inf
+    assert status(lambda: gp.phase_gradient_batch(phi)) == 1
+    # the context is still usable
+    out, st = gp.forward()
+    assert st["status"] == 0 and np.all(np.isfinite(out))
