@@ -1440,7 +1440,8 @@ int fl_problem_create(fl_ctx* ctx, int nt, int m, const double* D, const double*
     // the single-CTA stepper covers M = 1 up to 2^14 (FP32 mode) / 2^13 (FP64
     // mode); larger transforms run on the multimode runtime's kernels
     pr->use_mm = m > 1 || ilog2i(nt) > (precision == FL_PRECISION_FP64 ? 13 : 14);
-    if (pr->use_mm && ((m > 1 && !mm_supported_modes(m)) || !mm_round_launcher(ilog2i(nt))))
+    if (pr->use_mm ? ((m > 1 && !mm_supported_modes(m)) || !mm_round_launcher(ilog2i(nt)))
+                   : !sm_launcher(precision == FL_PRECISION_FP64, ilog2i(nt)))
         return set_err(ctx, FL_EUNSUPPORTED, "built shapes: M = 1 with Nt = 2^6..2^15, "
                        "M = 2..10 with Nt = 2^6..2^15 (got M = %d, Nt = %d)", m, nt);
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
