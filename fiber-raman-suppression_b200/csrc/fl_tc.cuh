@@ -103,8 +103,10 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
     unsigned char* Alo = Ahi + TS::A_BYTES;
     unsigned char* Bhi = Alo + TS::A_BYTES;
     unsigned char* Blo = Bhi + TS::B_BYTES;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // MMA completion
+    uint64_t* bbar = mbar + 1;                                         // B-image arrival
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
+    uint32_t* bfail = tmem_slot + 1;                                   // B copy timed out
 
     // ---- tensor memory and barrier
     if (warp == 0) {
@@ -113,18 +115,32 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
                      "r"(128));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
+    // ---- B = G rows (ij) x pairs, split hi/lo: the image prepared once per
+    // problem in exactly this shared-memory layout (B_hi then B_lo), brought in
+    // by the TMA engine as bulk copies (16-byte aligned, sizes multiples of 16)
+    // completing on bbar, while the threads build the first A tile
+    constexpr uint32_t kBBytes = 2 * TS::B_BYTES, kBChunk = 16384;
+    static_assert(kBBytes % 16 == 0, "bulk copy size");
     if (tid == 0) {
+        *bfail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
-        asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                         smem_u32(bbar)),
+                     "r"(kBBytes)
+                     : "memory");
+        const char* src = reinterpret_cast<const char*>(d.Gtc);
+        for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
+            const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                "[%3];" ::"r"(smem_u32(Bhi) + off),
+                "l"(src + off), "r"(n), "r"(smem_u32(bbar))
+                : "memory");
+        }
     }
-
-    // ---- B = G rows (ij) x pairs, split hi/lo: a copy of the image prepared
-    // once per problem in exactly this shared-memory layout (B_hi then B_lo)
-    {
-        const int4* src = reinterpret_cast<const int4*>(d.Gtc);
-        int4* dst = reinterpret_cast<int4*>(Bhi);
-        for (int e = tid; e < 2 * TS::B_BYTES / 16; e += kTcRows) dst[e] = __ldg(src + e);
-    }
+    bool b_waited = false;  // thread 0: the B image has been waited for
 
     const float* sq = static_cast<const float*>(d.sq);
     const cx<float>* ut = static_cast<const cx<float>*>(d.ut);
@@ -159,8 +175,23 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tmem = *tmem_slot;
 
-        // ---- 3 x KP/8 MMAs from one thread, committed to the barrier
-        if (tid == 0) {
+        // ---- 3 x KP/8 MMAs from one thread, committed to the barrier (after a
+        // bounded wait for the B image on the first tile; if it does not land
+        // the tile is flagged and no MMA is issued)
+        if (tid == 0 && !b_waited) {
+            uint32_t got = 0;
+            for (long it = 0; it < (1L << 26) && !got; it++) {
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}\n"
+                    : "=r"(got)
+                    : "r"(smem_u32(bbar))
+                    : "memory");
+            }
+            b_waited = true;
+            if (!got) *bfail = 1;
+        }
+        if (tid == 0 && !*bfail) {
             constexpr uint32_t idesc = tc_idesc(NN);
             const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
             const uint32_t b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
@@ -185,11 +216,12 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
                     "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
                     "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
             }
+        }
+        if (tid == 0)  // arrives once the MMAs above (if any) have completed
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                     smem_u32(mbar))
                 : "memory");
-        }
 
         // ---- bounded wait for this tile's MMAs (the barrier's current phase)
         uint32_t done = 0;
@@ -227,6 +259,7 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
         // the next tile's MMAs overwrite the accumulator and A: all reads done first
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
+        ok = ok && !*bfail;
 
         // ---- η_i = Σ_j δ_ij u_j
         cx<float> u[M];
@@ -244,6 +277,19 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
         }
     }
 
+    // ---- a B copy not waited for (no tile) or timed out may still be in
+    // flight: wait for it (bounded) before the CTA's shared memory is released
+    if (tid == 0 && (!b_waited || *bfail)) {
+        uint32_t got = 0;
+        for (long it = 0; it < (1L << 26) && !got; it++) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(got)
+                : "r"(smem_u32(bbar))
+                : "memory");
+        }
+    }
     // ---- release tensor memory
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
