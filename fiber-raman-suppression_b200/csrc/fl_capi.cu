@@ -444,8 +444,12 @@ struct MmWork {
     double* d_uL = nullptr;
     double* d_zsave = nullptr;
     unsigned char* d_mask = nullptr;
+    // mm_run's batch of evaluation rounds as a CUDA graph, for graph_nactive slots
+    cudaGraphExec_t graph = nullptr;
+    int graph_nactive = -1;
 
     ~MmWork() {
+        if (graph) cudaGraphExecDestroy(graph);
         cudaFree(pool);
         cudaFree(d_desc);
         cudaFree(d_state);
@@ -625,18 +629,54 @@ int mm_run(fl_problem* pr, MmWork* w, int nactive) {
     CU(mm_launch_control(a, 0));
     ctx->launches++;
     const int per_batch = 8;
-    const long max_rounds = 4 * 7 * (ctx->opts.max_iters + 2) + 64;
-    long rounds = 0;
-    for (;;) {
+    // one batch: 8 evaluation rounds, the counter of finished slots reset
+    // before the last round (which counts them)
+    auto enqueue_batch = [&]() -> cudaError_t {
         for (int r = 0; r < per_batch; r++) {
             a.ndone = nullptr;
             if (r == per_batch - 1) {
-                CU(cudaMemsetAsync(w->d_ndone, 0, sizeof(int), ctx->stream));
+                const cudaError_t e = cudaMemsetAsync(w->d_ndone, 0, sizeof(int), ctx->stream);
+                if (e != cudaSuccess) return e;
                 a.ndone = w->d_ndone;
             }
-            CU(round(a));
-            ctx->launches += a.fp64 ? 7 : 10;
+            const cudaError_t e = round(a);
+            if (e != cudaSuccess) return e;
         }
+        return cudaSuccess;
+    };
+    // The batch is captured once as a CUDA graph and replayed: each kernel
+    // reads every slot's phase from device memory, so the same launches serve
+    // every batch, and a batch costs one graph launch instead of 8 x 7..10
+    // kernel launches.  Capture is thread-local (other host threads, e.g. a
+    // server's, keep launching).
+    if (!w->graph || w->graph_nactive != nactive) {
+        if (w->graph) cudaGraphExecDestroy(w->graph);
+        w->graph = nullptr;
+        w->graph_nactive = -1;
+        cudaGraph_t g = nullptr;
+        CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e1 = enqueue_batch();
+        const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+        if (e1 != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return set_err(ctx, FL_ECUDA, "capturing the evaluation batch: %s",
+                           cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        }
+        const cudaError_t e3 = cudaGraphInstantiate(&w->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) {
+            w->graph = nullptr;
+            return set_err(ctx, FL_ECUDA, "instantiating the evaluation batch: %s",
+                           cudaGetErrorString(e3));
+        }
+        w->graph_nactive = nactive;
+    }
+    const long max_rounds = 4 * 7 * (ctx->opts.max_iters + 2) + 64;
+    long rounds = 0;
+    for (;;) {
+        CU(cudaGraphLaunch(w->graph, ctx->stream));
+        ctx->launches += per_batch * (a.fp64 ? 7 : 10);
         rounds += per_batch;
         CU(cudaMemcpyAsync(w->h_ndone, w->d_ndone, sizeof(int), cudaMemcpyDeviceToHost,
                            ctx->stream));
