@@ -950,7 +950,9 @@ struct SrvChunk {
     size_t bytes = 0;
     std::vector<SlotState> hs;
     std::vector<MmState> hms;
+    cudaGraphExec_t graph = nullptr;   // multimode: one launch's rounds, captured once
     ~SrvChunk() {
+        if (graph) cudaGraphExecDestroy(graph);
         delete w;
         delete mw;
         cudaFree(d_masks);
@@ -1202,8 +1204,31 @@ int srv_launch(fl_server* sv, SrvBucket* b, SrvChunk* c) {
         a.ndone = nullptr;
         a.stream = c->stream;
         MmRoundFn round = mm_round_launcher(logn);
-        CU(mm_launch_control(a, 0));  // prepares newly admitted slots (idempotent for the rest)
-        for (int r = 0; r < sv->opts.evals_per_launch; r++) CU(round(a));
+        // control (prepares newly admitted slots, idempotent for the rest) and
+        // evals_per_launch rounds over all the chunk's slots (finished ones are
+        // skipped by the kernels): the same launches every time, so they are
+        // captured once per chunk as a CUDA graph and replayed
+        if (!c->graph) {
+            cudaGraph_t g = nullptr;
+            CU(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e1 = mm_launch_control(a, 0);
+            for (int r = 0; e1 == cudaSuccess && r < sv->opts.evals_per_launch; r++) e1 = round(a);
+            const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            if (e1 != cudaSuccess || e2 != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return set_err(ctx, FL_ECUDA, "capturing a server launch: %s",
+                               cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+            }
+            const cudaError_t e3 = cudaGraphInstantiate(&c->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (e3 != cudaSuccess) {
+                c->graph = nullptr;
+                return set_err(ctx, FL_ECUDA, "instantiating a server launch: %s",
+                               cudaGetErrorString(e3));
+            }
+        }
+        CU(cudaGraphLaunch(c->graph, c->stream));
         sv->launches += 1 + (long)sv->opts.evals_per_launch * (a.fp64 ? 7 : 10);
     } else {
         LaunchFn fn = sm_launcher(b->precision == FL_PRECISION_FP64, logn);
