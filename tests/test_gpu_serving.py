@@ -148,3 +148,27 @@ def test_serving_multimode_requests(gpu_ctx):
     out_sm, _ = GPUProblem(gpu_ctx, smL).forward(P.serving_launch(sm, 0.1))
     assert np.array_equal(out_sm[-1], hs.out_field)
     srv.close()
+
+
+def test_serving_request_keeps_objective_of_submission(gpu_ctx):
+    # a band-gradient request computes the objective its problem had when it
+    # was submitted (fl_problem_set_objective), on the device, as the plain
+    # batched call does
+    fp = P.serving_grid_problem(2048)
+    gp = GPUProblem(gpu_ctx, fp)
+    phi = 0.4 * np.random.default_rng(6).standard_normal(fp.nt)
+    u0 = P.serving_launch(fp, 0.2)
+    short = P.FiberProblem(**{**fp.__dict__})
+    short.L = 0.3
+    ref = GPUProblem(gpu_ctx, short)
+    ref.set_objective("raman_peak")
+    Jp, gpk, _ = ref.phase_gradient_batch(phi[None, :], u0=u0)
+    srv = Server(gpu_ctx)
+    gp.set_objective("raman_peak")
+    h = srv.submit_band_gradient(gp, phi, u0=u0, L=0.3)
+    gp.set_objective("raman_band")      # later changes do not reach the request
+    srv.wait(h)
+    assert h.status == 0
+    assert abs(h.J - Jp[0]) <= 1e-9 * abs(Jp[0])
+    assert rel(h.out_grad, gpk[0]) < GRAD_TOL
+    srv.close()
