@@ -851,6 +851,123 @@ static int tsit5_solve(rhs_fn f, void *ctx, size_t n, const cplx *u0, double t0,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Pump-gain propagation (simulate_disp_gain_mmf.jl, gain_simulation/gain.jl) */
+/* ------------------------------------------------------------------------ */
+
+/* compute_gain: g(w) per bin into gw, returns the pump gain g_P.  The YDFA
+ * branch is calculate_gain_YDFA (gain.jl:150-166) on the PSD of
+ * psd_from_uw (gain.jl:122-127): the sums over bins do not depend on the bin
+ * order, so everything stays in FFT order. */
+static double gain_profile(const orc_gain *g, int nt, const cplx *uw, double Pp, double *gw) {
+    if (g->kind == 0) {
+        for (int b = 0; b < nt; b++) gw[b] = g->g_const;
+        return -1.0;
+    }
+    double W12 = 0.0, W21 = 0.0;
+    for (int b = 0; b < nt; b++) {
+        const double a = cabs(uw[b]);
+        const double Ps = a * a * g->psd_scale;
+        W12 += g->gamma_s * g->sigma_as[b] * Ps * g->df / (g->h_nu_s[b] * g->area);
+        W21 += g->gamma_s * g->sigma_es[b] * Ps * g->df / (g->h_nu_s[b] * g->area);
+    }
+    const double R12 = g->gamma_p * g->sigma_ap * Pp / (g->h_nu_p * g->area);
+    const double R21 = g->gamma_p * g->sigma_ep * Pp / (g->h_nu_p * g->area);
+    const double n2 = (R12 + W12) / (R12 + R21 + W12 + W21 + 1.0 / g->tau21);
+    const double n1 = 1.0 - n2;
+    for (int b = 0; b < nt; b++)
+        gw[b] = g->gamma_s * (g->sigma_es[b] * n2 - g->sigma_as[b] * n1) * g->rho;
+    return g->gamma_p * (g->sigma_ep * n2 - g->sigma_ap * n1) * g->rho;
+}
+
+typedef struct {
+    workspace w;
+    const orc_gain *g;
+    cplx *uw;
+    double *gw;
+} gain_ctx;
+
+static void gain_rhs_cb(void *ctx, double z, const cplx *u, cplx *du) {
+    gain_ctx *c = (gain_ctx *)ctx;
+    const orc_problem *p = c->w.p;
+    const int nt = p->nt;
+    const cplx *ut = u + 1;
+    /* compute_gain takes the lab-frame field e^{iDz} u~ and the pump power */
+    for (int b = 0; b < nt; b++) {
+        const double a = p->D[b] * z;
+        c->uw[b] = (cos(a) + I * sin(a)) * ut[b];
+    }
+    const double gP = gain_profile(c->g, nt, c->uw, creal(u[0]), c->gw);
+    rhs_forward_ws(&c->w, z, ut, du + 1);
+    for (int b = 0; b < nt; b++) du[1 + b] += 0.5 * c->gw[b] * ut[b];
+    du[0] = gP * u[0];
+}
+
+static int gain_ctx_init(gain_ctx *c, const orc_problem *p, const orc_gain *g) {
+    memset(c, 0, sizeof(*c));
+    if (!problem_valid(p) || p->m != 1 || !g || (g->kind != 0 && g->kind != 1)) return ORC_EINVAL;
+    if (g->kind == 1 && (!g->sigma_as || !g->sigma_es || !g->h_nu_s)) return ORC_EINVAL;
+    if (ws_init(&c->w, p, 0)) return ORC_ENOMEM;
+    c->g = g;
+    c->uw = (cplx *)malloc(sizeof(cplx) * p->nt);
+    c->gw = (double *)malloc(sizeof(double) * p->nt);
+    if (!c->uw || !c->gw) return ORC_ENOMEM;
+    return ORC_OK;
+}
+
+static void gain_ctx_free(gain_ctx *c) {
+    ws_free(&c->w);
+    free(c->uw);
+    free(c->gw);
+}
+
+int orc_rhs_gain(const orc_problem *p, const orc_gain *g, double z, const orc_c64 *state,
+                 orc_c64 *dstate) {
+    gain_ctx c;
+    int rc = gain_ctx_init(&c, p, g);
+    if (rc == ORC_OK) gain_rhs_cb(&c, z, (const cplx *)state, (cplx *)dstate);
+    gain_ctx_free(&c);
+    return rc;
+}
+
+int orc_forward_gain(const orc_problem *p, const orc_gain *g, double pump0,
+                     const orc_c64 *u0, orc_c64 *out_uwL, double *pump_L, orc_stats *st) {
+    gain_ctx c;
+    int rc = gain_ctx_init(&c, p, g);
+    const int nt = p ? p->nt : 0;
+    cplx *s0 = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * (nt + 1)) : NULL;
+    cplx *sL = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * (nt + 1)) : NULL;
+    if (rc == ORC_OK && (!s0 || !sL)) rc = ORC_ENOMEM;
+    orc_stats local;
+    if (!st) st = &local;
+    if (rc == ORC_OK) {
+        /* u0 = vcat(Pp0, u_w0) (simulate_disp_gain_mmf.jl:218-219) */
+        s0[0] = pump0;
+        for (int b = 0; b < nt; b++) {
+            s0[1 + b] = u0[b].re + I * u0[b].im;
+            if (!isfinite(u0[b].re) || !isfinite(u0[b].im)) rc = ORC_NONFINITE;
+        }
+    }
+    if (rc == ORC_OK)
+        rc = tsit5_solve(gain_rhs_cb, &c, (size_t)nt + 1, s0, 0.0, p->L, p->reltol, p->abstol,
+                         sL, st, NULL);
+    if (rc == ORC_OK && st->z_end != p->L) rc = ORC_EINVAL;
+    if (rc == ORC_OK) {
+        if (pump_L) *pump_L = creal(sL[0]);
+        if (out_uwL)
+            for (int b = 0; b < nt; b++) {
+                const double a = p->D[b] * p->L;
+                const cplx y = (cos(a) + I * sin(a)) * sL[1 + b];
+                out_uwL[b].re = creal(y);
+                out_uwL[b].im = cimag(y);
+            }
+    }
+    free(s0);
+    free(sL);
+    gain_ctx_free(&c);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Drivers                                                                   */
 /* ------------------------------------------------------------------------ */
 

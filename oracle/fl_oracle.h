@@ -83,6 +83,36 @@ void orc_dense_free(orc_dense *d);
 int orc_adjoint(const orc_problem *p, const orc_dense *fwd,
                 const orc_c64 *lambdaL, orc_c64 *lambda0, orc_stats *st);
 
+/* Gain model of the pump-gain propagation (simulate_disp_gain_mmf.jl:68-102,
+ * gain_simulation/gain.jl:25-166).  kind 0: constant gain g_const per metre
+ * on every bin, pump gain -1 (the reference's placeholder); kind 1: the
+ * Yb-doped fiber steady-state rate equations with the caller's cross
+ * sections.  Per-bin arrays are in FFT bin order (the physical-order arrays
+ * ifftshift-ed). */
+typedef struct {
+    int kind;
+    double g_const;
+    double gamma_p, sigma_ap, sigma_ep, h_nu_p;   /* pump overlap, cross sections [m^2], h nu_p [J] */
+    double gamma_s, area, rho, tau21;             /* signal overlap, core area [m^2], ions [m^-3], lifetime [s] */
+    double psd_scale;                             /* |u_w|^2 -> W/Hz: (Nt dt)^2 x repetition rate */
+    double df;                                    /* bin width [Hz] */
+    const double *sigma_as, *sigma_es;            /* Nt signal cross sections [m^2] */
+    const double *h_nu_s;                         /* Nt photon energies [J] */
+} orc_gain;
+
+/* One evaluation of the pump-gain RHS (disp_gain_smf!,
+ * simulate_disp_gain_mmf.jl:21-66) for M = 1: state (Nt + 1) complex values
+ * [P_pump; u~]; dP/dz = g_P P, du~/dz = (disp_mmf! RHS) + g(w)/2 u~. */
+int orc_rhs_gain(const orc_problem *p, const orc_gain *g, double z, const orc_c64 *state,
+                 orc_c64 *dstate);
+
+/* Pump-gain Tsit5 solve 0 -> L (solve_disp_gain_smf,
+ * simulate_disp_gain_mmf.jl:204-239; the reference fixes reltol = 1e-5 and
+ * keeps the default abstol: set them in p).  out_uwL receives the lab-frame
+ * spectrum at L, pump_L the pump power there. */
+int orc_forward_gain(const orc_problem *p, const orc_gain *g, double pump0,
+                     const orc_c64 *u0, orc_c64 *out_uwL, double *pump_L, orc_stats *st);
+
 /* Fixed-step RK4 scalar restatement (scalar_crosscheck.jl:38-67). */
 int orc_rk4_scalar(const orc_problem *p, const orc_c64 *u0, int steps,
                    orc_c64 *out);

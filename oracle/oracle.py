@@ -30,6 +30,14 @@ RETCODES = {0: "ok", 1: "invalid argument", 2: "non-finite value", 3: "dt underf
             4: "maxiters", 5: "out of memory", 6: "gamma not permutation-symmetric"}
 
 
+class OrcGain(C.Structure):
+    _fields_ = [("kind", C.c_int), ("g_const", C.c_double), ("gamma_p", C.c_double),
+                ("sigma_ap", C.c_double), ("sigma_ep", C.c_double), ("h_nu_p", C.c_double),
+                ("gamma_s", C.c_double), ("area", C.c_double), ("rho", C.c_double),
+                ("tau21", C.c_double), ("psd_scale", C.c_double), ("df", C.c_double),
+                ("sigma_as", C.c_void_p), ("sigma_es", C.c_void_p), ("h_nu_s", C.c_void_p)]
+
+
 class OracleError(RuntimeError):
     def __init__(self, rc):
         super().__init__(f"oracle error {rc}: {RETCODES.get(rc, '?')}")
@@ -200,3 +208,55 @@ def phase_gradient(fp, phase):
     if failed:
         raise OracleError(2)
     return float(J[0]), g[0], int(ns[0])
+
+
+def _gain_struct(gain):
+    """orc_gain from a constant gain [1/m] or a YDFAParams (the arrays are
+    kept alive on the returned holder)."""
+    from fiberlab_gpu import gain as G
+    g = OrcGain()
+    keep = []
+    if isinstance(gain, (int, float)):
+        g.kind, g.g_const = 0, float(gain)
+    else:
+        a = G.gain_struct_arrays(gain)
+        g.kind = 1
+        for k in ("gamma_p", "sigma_ap", "sigma_ep", "h_nu_p", "gamma_s", "area", "rho",
+                  "tau21", "psd_scale", "df"):
+            setattr(g, k, float(a[k]))
+        for k in ("sigma_as", "sigma_es", "h_nu_s"):
+            arr = np.ascontiguousarray(a[k], dtype=np.float64)
+            keep.append(arr)
+            setattr(g, k, arr.ctypes.data)
+    return g, keep
+
+
+def rhs_gain(fp, gain, z, pump, u):
+    """One pump-gain RHS evaluation (orc_rhs_gain): returns (dP/dz, du~/dz)."""
+    pr = Problem(fp)
+    g, keep = _gain_struct(gain)
+    st = _c(np.concatenate([[complex(pump)], np.asarray(u, np.complex128).reshape(-1)]))
+    out = np.empty_like(st)
+    rc = lib().orc_rhs_gain(C.byref(pr.s), C.byref(g), C.c_double(z),
+                            C.c_void_p(st.ctypes.data), C.c_void_p(out.ctypes.data))
+    if rc:
+        raise OracleError(rc)
+    return out[0], out[1:].reshape(1, -1)
+
+
+def forward_gain(fp, gain, pump0, u0=None):
+    """Pump-gain solve 0 -> L (orc_forward_gain): (lab-frame u(L) (1, Nt),
+    pump power at L, stats)."""
+    pr = Problem(fp)
+    g, keep = _gain_struct(gain)
+    u0 = _c(fp.uw0 if u0 is None else u0)
+    out = np.empty(fp.nt, np.complex128)
+    pl = C.c_double()
+    st = OrcStats()
+    rc = lib().orc_forward_gain(C.byref(pr.s), C.byref(g), C.c_double(pump0),
+                                C.c_void_p(u0.ctypes.data), C.c_void_p(out.ctypes.data),
+                                C.byref(pl), C.byref(st))
+    if rc:
+        raise OracleError(rc)
+    return out.reshape(1, -1), pl.value, {"naccept": st.naccept, "nreject": st.nreject,
+                                          "nf": st.nf, "z_end": st.z_end}
