@@ -434,3 +434,33 @@ def test_boundary_rejects_bad_input(gpu_ctx):
     # the context is still usable
     out, st = gp.forward()
     assert st["status"] == 0 and np.all(np.isfinite(out))
+
+
+def test_reference_dict_interface(gpu_ctx):
+    # solve_disp_mmf(uω0, fiber, sim) / solve_adjoint_disp_mmf(λωL, sol, fiber,
+    # sim) as the reference's callers use them (propagation.jl:35-53,
+    # physics_models.jl:1035-1041): sol(z) at stored positions, "uω_z" and
+    # "ut_z" at fiber["zsave"], destats, and sol_adj(0) = λ(0)
+    from fiberlab_gpu import solve as S
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    zs = [0.1, 0.25]
+    fiber = {"Dω": fp.D, "γ": fp.gamma, "hRω": fp.hR, "one_m_fR": fp.one_m_fR, "L": fp.L,
+             "zsave": zs}
+    res = S.solve_disp_mmf(fp.uw0, fiber, fp.sim, ctx=gpu_ctx)
+    sol = res["ode_sol"]
+    assert sol.retcode == "Success" and sol.destats.naccept > 0
+    assert sol.destats.nf == 3 + 6 * (sol.destats.naccept + sol.destats.nreject)
+    ref, _, dense = O.forward(fp, zsave=[0.0] + zs + [fp.L], keep_dense=True)
+    for i in range(len(zs)):
+        assert rel(res["uω_z"][i], ref[1 + i]) < FIELD_TOL_FP32
+    assert np.allclose(res["ut_z"], np.fft.fft(res["uω_z"], axis=-1), rtol=0, atol=0)
+    uL = np.exp(1j * fp.D * fp.L) * sol(fp.L)   # lab frame from the interaction frame
+    assert rel(uL, ref[-1]) < FIELD_TOL_FP32
+    with pytest.raises(P.ArgumentError):
+        sol(0.3)
+    _, seed = P.band_cost_and_seed(uL, fp.mask)
+    sol_adj = S.solve_adjoint_disp_mmf(seed, sol, fiber, fp.sim)
+    lref, _ = O.adjoint(fp, dense, seed)
+    assert rel(sol_adj(0.0), lref) < GRAD_TOL
+    assert sol_adj.destats.naccept > 0
