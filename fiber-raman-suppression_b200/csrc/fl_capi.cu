@@ -1551,6 +1551,134 @@ int fl_problem_destroy(fl_problem* pr) {
     return FL_OK;
 }
 
+int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, const double* u0,
+                    double* out_uwL, double* pump_L, fl_stats* stats) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!gain || !u0 || !out_uwL) return set_err(ctx, FL_EINVAL, "null argument");
+    const int nt = pr->nt, logn = ilog2i(nt);
+    if (pr->m != 1 || pr->precision != FL_PRECISION_FP32 || !gain_built(logn))
+        return set_err(ctx, FL_EUNSUPPORTED,
+                       "gain propagation is built for M = 1 in FP32 mode at Nt = 2^6..2^13");
+    if (gain->kind != FL_GAIN_CONSTANT && gain->kind != FL_GAIN_YDFA)
+        return set_err(ctx, FL_EINVAL, "unknown gain model %d", gain->kind);
+    if (!std::isfinite(pump_power)) return set_err(ctx, FL_EINVAL, "pump power must be finite");
+    // the gain tables: W12/W21 weights and the g(ω) coefficients per bin
+    std::vector<double> tab(4 * (size_t)nt, 0.0);
+    double r12c = 0, r21c = 0, inv_tau = 0, gpe = 0, gpa = 0;
+    if (gain->kind == FL_GAIN_CONSTANT) {
+        if (!std::isfinite(gain->g_const)) return set_err(ctx, FL_EINVAL, "gain must be finite");
+    } else {
+        const fl_gain& g = *gain;
+        if (!g.sigma_as || !g.sigma_es || !g.h_nu_s)
+            return set_err(ctx, FL_EINVAL, "YDFA gain needs the per-bin cross sections");
+        const double sc[] = {g.gamma_p, g.sigma_ap, g.sigma_ep, g.h_nu_p, g.gamma_s, g.area,
+                             g.rho, g.tau21, g.psd_scale, g.df};
+        for (double x : sc)
+            if (!(std::isfinite(x) && x >= 0)) return set_err(ctx, FL_EINVAL, "YDFA parameters must be finite and nonnegative");
+        if (!(g.h_nu_p > 0 && g.area > 0 && g.tau21 > 0))
+            return set_err(ctx, FL_EINVAL, "YDFA photon energy, area and lifetime must be positive");
+        for (int b = 0; b < nt; b++) {
+            if (!(std::isfinite(g.sigma_as[b]) && g.sigma_as[b] >= 0 && std::isfinite(g.sigma_es[b]) &&
+                  g.sigma_es[b] >= 0 && g.h_nu_s[b] > 0 && std::isfinite(g.h_nu_s[b])))
+                return set_err(ctx, FL_EINVAL, "YDFA cross sections and photon energies must be finite");
+            const double w = g.gamma_s * g.psd_scale * g.df / (g.h_nu_s[b] * g.area);
+            tab[b] = w * g.sigma_as[b];                      // W12 weight
+            tab[nt + b] = w * g.sigma_es[b];                 // W21 weight
+            tab[2 * (size_t)nt + b] = g.gamma_s * g.sigma_as[b] * g.rho;  // sA
+            tab[3 * (size_t)nt + b] = g.gamma_s * g.sigma_es[b] * g.rho;  // sE
+        }
+        r12c = g.gamma_p * g.sigma_ap / (g.h_nu_p * g.area);
+        r21c = g.gamma_p * g.sigma_ep / (g.h_nu_p * g.area);
+        inv_tau = 1.0 / g.tau21;
+        gpe = g.gamma_p * g.sigma_ep * g.rho;
+        gpa = g.gamma_p * g.sigma_ap * g.rho;
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < 2 * nt; i++) {
+        if (!std::isfinite(u0[i])) return set_err(ctx, FL_EINVAL, "input spectrum must be finite");
+        nrm += u0[i] * u0[i];
+    }
+    if (!(nrm > 0)) return set_err(ctx, FL_EINVAL, "input spectrum must be nonzero");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    // one device area: launch, two states, seven FP32 stages, two scratch
+    // fields, error partial and weights, output, gain tables, descriptor, result
+    const size_t F = 16 * (size_t)nt, H = 8 * (size_t)nt;
+    const size_t bytes = F * 4 + H * 7 + F * 2 + F + H + 4 * H + sizeof(GainDesc) + sizeof(GainOut) + 256;
+    char* pool = nullptr;
+    CU(cudaMalloc(&pool, bytes));
+    char* p = pool;
+    auto take = [&](size_t n) { char* q = p; p += (n + 255) & ~size_t(255); return q; };
+    GainDesc hd;
+    memset(&hd, 0, sizeof hd);
+    SlotDesc& d = hd.s;
+    d.Dturns = pr->d_Dturns;
+    d.Heff[0] = pr->d_Heff[0];
+    d.ss[0] = pr->d_ss[0];
+    d.tw[0] = pr->d_tw[0];   // FP32 twiddles only (no FP64 stage here)
+    d.gamma = pr->gamma0;
+    d.one_m_fR = pr->one_m_fR;
+    d.L = pr->L;
+    d.reltol = pr->reltol;
+    d.abstol = pr->abstol;
+    d.mode = MODE_FORWARD;
+    d.max_iters = ctx->opts.max_iters;
+    double* d_u0 = (double*)take(F);
+    d.u0 = d_u0;
+    d.u[0] = (double*)take(F);
+    d.u[1] = (double*)take(F);
+    d.uL_out = (double*)take(F);
+    for (int i = 0; i < 7; i++) d.kf[i] = take(H);
+    d.scr[0] = take(F);
+    d.scr[1] = take(F);
+    d.esv = (double*)take(F);
+    d.skv = (double*)take(H);
+    double* d_tab = (double*)take(4 * H);
+    hd.kind = gain->kind;
+    hd.g_const = gain->g_const;
+    hd.r12c = r12c;
+    hd.r21c = r21c;
+    hd.inv_tau = inv_tau;
+    hd.gpe = gpe;
+    hd.gpa = gpa;
+    hd.wa = d_tab;
+    hd.we = d_tab + nt;
+    hd.sA = d_tab + 2 * (size_t)nt;
+    hd.sE = d_tab + 3 * (size_t)nt;
+    hd.pump0 = pump_power;
+    GainDesc* d_desc = (GainDesc*)take(sizeof(GainDesc));
+    GainOut* d_out = (GainOut*)take(sizeof(GainOut));
+    GainOut ho{};
+    cudaError_t e = cudaMemcpyAsync(d_u0, u0, F, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tab, tab.data(), 4 * H, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_desc, &hd, sizeof hd, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
+    if (e == cudaSuccess) e = launch_gain(logn, d_desc, d_out, ctx->stream);
+    if (e == cudaSuccess) ctx->launches++;
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&ho, d_out, sizeof ho, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out_uwL, d.uL_out, F, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(pool);
+    if (e != cudaSuccess) return set_err(ctx, FL_ECUDA, "gain propagation: %s", cudaGetErrorString(e));
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->naccept = ho.naccept;
+        stats->nreject = ho.nreject;
+        stats->nf = ho.nf;
+        stats->status = ho.status;
+        stats->z_end = ho.z_end;
+    }
+    if (pump_L) *pump_L = ho.pump_L;
+    if (ho.status) return set_err(ctx, ho.status, "%s", fl_status_string(ho.status));
+    return FL_OK;
+}
+
 int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave,
                double* out_spectra, fl_stats* stats) {
     int rc = check_problem(pr);

@@ -35,4 +35,10 @@ LaunchFn sm_launcher(int fp64, int logn);
 // threads per CTA of a built launcher (0 when not built)
 int sm_threads(int fp64, int logn);
 
+// pump-gain forward solve of one single-mode problem (FP32 right-hand side,
+// FP64 state and error norm), run to completion in one launch; false / an
+// error when log2 Nt is not built (2^6..2^13)
+bool gain_built(int logn);
+cudaError_t launch_gain(int logn, const GainDesc* desc, GainOut* out, cudaStream_t stream);
+
 }  // namespace fl

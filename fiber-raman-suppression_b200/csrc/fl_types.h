@@ -179,4 +179,28 @@ struct MmState {
     long iters, a_iters;
 };
 
+// ---------------------------------------------------------------------------
+// Pump-gain single-mode forward solve (disp_gain_smf!, forward only): the
+// stepper's slot descriptor (tables, launch u0, state u[2], stages kf[7],
+// scratch scr[2], error buffers esv/skv) plus the gain model.  The state is
+// [P_pump; ũ]; g(ω) multiplies ũ/2 and dP/dz = g_P P.
+struct GainDesc {
+    SlotDesc s;
+    int kind;               // 0 constant gain, 1 Yb-doped fiber rate equations
+    double g_const;         // constant model: g per metre on every bin (g_P = -1)
+    double r12c, r21c;      // rate equations: R12 = r12c P, R21 = r21c P
+    double inv_tau;         // 1 / τ21
+    double gpe, gpa;        // g_P = gpe n2 - gpa n1
+    const double* wa;       // W12 = Σ_b wa[b] |u_b|², W21 = Σ_b we[b] |u_b|² (FFT bin order)
+    const double* we;
+    const double* sA;       // g_b = sE[b] n2 - sA[b] n1
+    const double* sE;
+    double pump0;           // P_pump at z = 0 [W]
+};
+struct GainOut {
+    long naccept, nreject, nf;
+    int status;
+    double z_end, pump_L;
+};
+
 }  // namespace fl

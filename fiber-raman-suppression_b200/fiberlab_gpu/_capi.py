@@ -28,7 +28,7 @@ EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_forward_noalloc", "fl_mode_phase_gradient_batch",
            "fl_mode_phase_gradient_batch_device", "fl_server_create", "fl_server_destroy",
            "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_info_get",
-           "fl_problem_set_objective")
+           "fl_problem_set_objective", "fl_forward_gain")
 
 # device objectives (FL_OBJ_*) by the reference's objective names
 # (physics_models.jl:947-962); temporal_width runs with a host seed
@@ -39,6 +39,15 @@ OBJECTIVE = {"raman_band": 0, "mode_sum": 0, "mmf_sum": 0, "fundamental_mode": 1
 class FlCtxOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("checkpoints", C.c_int),
                 ("segment_steps", C.c_int), ("step_log", C.c_int), ("max_iters", C.c_long)]
+
+
+class FlGain(C.Structure):
+    """fl_gain: the gain model of fl_forward_gain."""
+    _fields_ = [("kind", C.c_int), ("g_const", C.c_double), ("gamma_p", C.c_double),
+                ("sigma_ap", C.c_double), ("sigma_ep", C.c_double), ("h_nu_p", C.c_double),
+                ("gamma_s", C.c_double), ("area", C.c_double), ("rho", C.c_double),
+                ("tau21", C.c_double), ("psd_scale", C.c_double), ("df", C.c_double),
+                ("sigma_as", C.c_void_p), ("sigma_es", C.c_void_p), ("h_nu_s", C.c_void_p)]
 
 
 class FlStats(C.Structure):
@@ -104,6 +113,8 @@ def load() -> C.CDLL:
                                           C.POINTER(vp)]
         lib.fl_problem_destroy.argtypes = [vp]
         lib.fl_problem_set_objective.argtypes = [vp, ip, dp]
+        lib.fl_forward_gain.argtypes = [vp, C.POINTER(FlGain), dp, vp, vp, C.POINTER(C.c_double),
+                                        C.POINTER(FlStats)]
         lib.fl_forward.argtypes = [vp, vp, vp, ip, vp, C.POINTER(FlStats)]
         lib.fl_adjoint.argtypes = [vp, vp, vp, C.POINTER(FlStats)]
         lib.fl_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
@@ -212,6 +223,34 @@ class GPUProblem:
         self.ctx.check(load().fl_problem_set_objective(self.h, OBJECTIVE[name],
                                                        float(worst_mode_tau)))
         self.objective = name
+
+    def forward_gain(self, gain, pump_power: float, u0=None):
+        """Pump-gain forward solve (fl_forward_gain): gain is a constant gain
+        [1/m] or a fiberlab_gpu.gain.YDFAParams; returns (lab-frame u(L)
+        (1, Nt), pump power at L, stats)."""
+        from . import gain as G
+        fp = self.fp
+        u0 = np.ascontiguousarray(fp.uw0 if u0 is None else u0, dtype=np.complex128)
+        g = FlGain()
+        keep = []
+        if isinstance(gain, (int, float)):
+            g.kind, g.g_const = 0, float(gain)
+        else:
+            a = G.gain_struct_arrays(gain)
+            g.kind = 1
+            for k in ("gamma_p", "sigma_ap", "sigma_ep", "h_nu_p", "gamma_s", "area", "rho",
+                      "tau21", "psd_scale", "df"):
+                setattr(g, k, float(a[k]))
+            for k in ("sigma_as", "sigma_es", "h_nu_s"):
+                arr = np.ascontiguousarray(a[k], dtype=np.float64)
+                keep.append(arr)
+                setattr(g, k, arr.ctypes.data)
+        out = np.empty((1, fp.nt), dtype=np.complex128)
+        pl = C.c_double()
+        st = FlStats()
+        self.ctx.check(load().fl_forward_gain(self.h, C.byref(g), float(pump_power), _ptr(u0),
+                                              _ptr(out), C.byref(pl), C.byref(st)))
+        return out, pl.value, st.as_dict()
 
     def forward(self, u0=None, saveat=None):
         fp = self.fp

@@ -125,6 +125,32 @@ int fl_problem_destroy(fl_problem *prob);
 #define FL_OBJ_RAMAN_PEAK 3  /* strongest in-band bin (summed over modes) over the total */
 int fl_problem_set_objective(fl_problem *prob, int objective, double worst_mode_tau);
 
+/* Pump-gain single-mode forward solve 0 -> L.  Replaces solve_disp_gain_smf
+ * (simulate_disp_gain_mmf.jl:204-239) with its right-hand side disp_gain_smf!
+ * (:21-66): the state [P_pump; ũ], dP/dz = g_P P, and disp_mmf!'s derivative
+ * plus g(ω) ũ / 2.  The gain is constant (FL_GAIN_CONSTANT: g_const per metre
+ * on every bin, g_P = -1, the reference's placeholder, :74-78) or the
+ * Yb-doped fiber steady-state rate equations (FL_GAIN_YDFA:
+ * calculate_gain_YDFA, gain_simulation/gain.jl:150-166, on the PSD
+ * |u_ω|² psd_scale of psd_from_uω, :122-127), whose per-bin arrays are in FFT
+ * bin order (the reference's physical-order arrays ifftshift-ed).  M = 1,
+ * FP32 mode, Nt = 2^6..2^13; the problem's reltol/abstol apply (the
+ * reference fixes reltol = 1e-5).  out_uwL receives the lab-frame spectrum at
+ * L (Nt complex), pump_L the pump power there; stats counts the attempts. */
+#define FL_GAIN_CONSTANT 0
+#define FL_GAIN_YDFA 1
+typedef struct {
+    int kind;                 /* FL_GAIN_CONSTANT or FL_GAIN_YDFA */
+    double g_const;           /* constant model: gain per metre */
+    double gamma_p, sigma_ap, sigma_ep, h_nu_p;  /* pump overlap, cross sections [m^2], h nu_p [J] */
+    double gamma_s, area, rho, tau21;            /* signal overlap, core area [m^2], ions [m^-3], [s] */
+    double psd_scale;         /* (Nt dt)^2 x repetition rate: |u_w|^2 -> W/Hz */
+    double df;                /* bin width [Hz] */
+    const double *sigma_as, *sigma_es, *h_nu_s; /* Nt each, FFT bin order (host memory) */
+} fl_gain;
+int fl_forward_gain(fl_problem *prob, const fl_gain *gain, double pump_power, const double *u0,
+                    double *out_uwL, double *pump_L, fl_stats *stats);
+
 /* Forward solve 0 -> L.  Replaces solve_disp_mmf (simulate_disp_mmf.jl:183-207)
  * as used by propagate (propagation.jl:89-123): out_spectra receives the
  * lab-frame spectra cis(D z) ũ(z) at each saveat position (Nt*M*nsave

@@ -464,3 +464,49 @@ def test_reference_dict_interface(gpu_ctx):
     lref, _ = O.adjoint(fp, dense, seed)
     assert rel(sol_adj(0.0), lref) < GRAD_TOL
     assert sol_adj.destats.naccept > 0
+
+
+def _synthetic_yb_sections():
+    # smooth Yb-like shapes: a 976 nm absorption peak, emission red of it
+    wl = np.linspace(900e-9, 1150e-9, 60)
+    sa = 2.5e-24 * np.exp(-((wl - 976e-9) / 8e-9) ** 2) + 6e-26 * np.exp(-((wl - 1030e-9) / 20e-9) ** 2)
+    se = 2.5e-24 * np.exp(-((wl - 976e-9) / 8e-9) ** 2) + 6e-25 * np.exp(-((wl - 1030e-9) / 25e-9) ** 2)
+    return (wl, sa), (wl, se)
+
+
+@pytest.mark.parametrize("model", ["constant", "ydfa"])
+def test_gain_propagation_matches_oracle(gpu_ctx, model):
+    # fl_forward_gain (solve_disp_gain_smf, simulate_disp_gain_mmf.jl:204-239):
+    # the state [P_pump; ũ] with the constant or the rate-equation gain
+    # against the oracle's restatement
+    from fiberlab_gpu import gain as G
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.05,
+                               rep_rate_hz=80e6, wavelength_m=1030e-9)
+    gain = 0.8 if model == "constant" else G.ydfa_params(fp.sim, *_synthetic_yb_sections())
+    out, pump_L, st = GPUProblem(gpu_ctx, fp).forward_gain(gain, 0.05)
+    ref, pump_ref, rst = O.forward_gain(fp, gain, 0.05)
+    assert st["status"] == 0 and st["z_end"] == fp.L
+    assert rel(out, ref) < FIELD_TOL_FP32
+    assert pump_L == pytest.approx(pump_ref, rel=1e-6)
+    assert st["nf"] == 3 + 6 * (st["naccept"] + st["nreject"])
+    assert abs(st["naccept"] - rst["naccept"]) <= 2
+
+
+def test_gain_reference_shape_and_limits(gpu_ctx):
+    # test_numerical_kernels.jl:5-25 at the smallest built grid (2^6): 1030 nm,
+    # 300 fs Gaussian 1e-4 W at 80 MHz, no nonlinearity or dispersion, 1e-5 m,
+    # 0.05 W pump, reltol 1e-5: succeeds with a finite field
+    from fiberlab_gpu import gain as G
+    fp = P.single_mode_problem(nt=64, time_window_ps=5.0, L=1e-5, power_w=1e-4, fwhm_s=300e-15,
+                               rep_rate_hz=80e6, gamma=0.0, betas=(0.0,), beta_order=2, fR=0.0,
+                               wavelength_m=1030e-9, pulse="gauss", reltol=1e-5)
+    gain = G.ydfa_params(fp.sim, *_synthetic_yb_sections())
+    gp = GPUProblem(gpu_ctx, fp)
+    out, pump_L, st = gp.forward_gain(gain, 0.05)
+    ref, pump_ref, _ = O.forward_gain(fp, gain, 0.05)
+    assert st["status"] == 0 and np.all(np.isfinite(out)) and np.isfinite(pump_L)
+    assert rel(out, ref) < FIELD_TOL_FP32
+    # built for M = 1, FP32 mode, Nt <= 2^13
+    with pytest.raises(FiberLabGPUError) as e:
+        GPUProblem(gpu_ctx, fp, "fp64").forward_gain(0.5, 0.05)
+    assert e.value.status == 10
