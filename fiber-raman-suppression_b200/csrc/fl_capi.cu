@@ -1552,11 +1552,22 @@ int fl_problem_destroy(fl_problem* pr) {
 }
 
 int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, const double* u0,
-                    double* out_uwL, double* pump_L, fl_stats* stats) {
+                    const double* saveat, int nsave, double* out_spectra, double* out_pump,
+                    fl_stats* stats) {
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
-    if (!gain || !u0 || !out_uwL) return set_err(ctx, FL_EINVAL, "null argument");
+    if (!gain || !u0 || !saveat || !out_spectra || !out_pump)
+        return set_err(ctx, FL_EINVAL, "null argument");
+    // propagation.jl:60-70: sorted, unique, starts at 0 and ends at L
+    if (nsave < 2) return set_err(ctx, FL_EINVAL, "saveat must include 0 and the fiber length");
+    for (int i = 0; i < nsave; i++) {
+        if (!std::isfinite(saveat[i])) return set_err(ctx, FL_EINVAL, "saveat distances must be finite");
+        if (i > 0 && !(saveat[i] > saveat[i - 1]))
+            return set_err(ctx, FL_EINVAL, "saveat distances must be sorted and unique");
+    }
+    if (saveat[0] != 0.0 || saveat[nsave - 1] != pr->L)
+        return set_err(ctx, FL_EINVAL, "saveat must start at 0 and end at the fiber length");
     const int nt = pr->nt, logn = ilog2i(nt);
     if (pr->m != 1 || pr->precision != FL_PRECISION_FP32 || !gain_built(logn))
         return set_err(ctx, FL_EUNSUPPORTED,
@@ -1605,7 +1616,8 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
     // one device area: launch, two states, seven FP32 stages, two scratch
     // fields, error partial and weights, output, gain tables, descriptor, result
     const size_t F = 16 * (size_t)nt, H = 8 * (size_t)nt;
-    const size_t bytes = F * 4 + H * 7 + F * 2 + F + H + 4 * H + sizeof(GainDesc) + sizeof(GainOut) + 256;
+    const size_t bytes = F * 4 + H * 7 + F * 2 + F + H + 4 * H + F * (size_t)nsave +
+                         16 * (size_t)nsave + sizeof(GainDesc) + sizeof(GainOut) + 4 * 256;
     char* pool = nullptr;
     CU(cudaMalloc(&pool, bytes));
     char* p = pool;
@@ -1635,6 +1647,11 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
     d.esv = (double*)take(F);
     d.skv = (double*)take(H);
     double* d_tab = (double*)take(4 * H);
+    double* d_zsave = (double*)take(8 * (size_t)nsave);
+    d.zsave = d_zsave;
+    d.nsave = nsave;
+    d.save_out = (double*)take(F * (size_t)nsave);
+    hd.pump_save = (double*)take(8 * (size_t)nsave);
     hd.kind = gain->kind;
     hd.g_const = gain->g_const;
     hd.r12c = r12c;
@@ -1654,6 +1671,8 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_tab, tab.data(), 4 * H, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_zsave, saveat, 8 * (size_t)nsave, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_desc, &hd, sizeof hd, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
     if (e == cudaSuccess) e = launch_gain(logn, d_desc, d_out, ctx->stream);
@@ -1662,7 +1681,11 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(&ho, d_out, sizeof ho, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(out_uwL, d.uL_out, F, cudaMemcpyDeviceToHost, ctx->stream);
+        e = cudaMemcpyAsync(out_spectra, d.save_out, F * (size_t)nsave, cudaMemcpyDeviceToHost,
+                            ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out_pump, hd.pump_save, 8 * (size_t)nsave, cudaMemcpyDeviceToHost,
+                            ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     cudaFree(pool);
     if (e != cudaSuccess) return set_err(ctx, FL_ECUDA, "gain propagation: %s", cudaGetErrorString(e));
@@ -1674,7 +1697,6 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
         stats->status = ho.status;
         stats->z_end = ho.z_end;
     }
-    if (pump_L) *pump_L = ho.pump_L;
     if (ho.status) return set_err(ctx, ho.status, "%s", fl_status_string(ho.status));
     return FL_OK;
 }

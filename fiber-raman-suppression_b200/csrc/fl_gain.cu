@@ -88,6 +88,15 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         io[s] = down<float>(x);
     }
     double pp = g.pump0;
+    // save positions at z = 0: the launch (the lab frame equals the interaction frame there)
+    int save_idx = 0;
+    while (save_idx < d.nsave && d.zsave[save_idx] == 0.0) {
+        double* o = d.save_out + (size_t)save_idx * 2 * N;
+#pragma unroll
+        for (int s = 0; s < E; s++) st2(o, Sol::bin(s), ld2(d.u0, Sol::bin(s)));
+        if (threadIdx.x == 0) g.pump_save[save_idx] = pp;
+        save_idx++;
+    }
     long nf = 0, naccept = 0, nreject = 0;
     int status = ST_OK;
     double kp[7];
@@ -213,6 +222,41 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         naccept++;
         double znew = z + dt;
         if (fabs(znew - L) < 100.0 * kEps * fmax(z, L)) znew = L;  // snap to the tstop
+        // save positions in (z, znew]: Tsit5's free interpolant
+        // u_n + dt Σ_i b_i(θ) k_i for the field and the pump power
+        while (save_idx < d.nsave && d.zsave[save_idx] <= znew && d.zsave[save_idx] > z) {
+            const double zs = d.zsave[save_idx], th = (zs - z) / dt;
+            double bi[7];
+            for (int i = 0; i < 7; i++) {
+                double b = 0.0, tp = th;
+                for (int q = 0; q < 4; q++) {
+                    b += kT5r[i][q] * tp;
+                    tp *= th;
+                }
+                bi[i] = b;
+            }
+            double* o = d.save_out + (size_t)save_idx * 2 * N;
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int b = Sol::bin(s);
+                double xr = 0.0, xi = 0.0;
+                for (int i = 0; i < 7; i++) {
+                    const CF ki = k[i][b];
+                    xr += bi[i] * (double)ki.re;
+                    xi += bi[i] * (double)ki.im;
+                }
+                const cx<double> un0 = ld2(u, b);
+                const cx<double> x = mk(un0.re + dt * xr, un0.im + dt * xi);
+                const cx<double> p = phasor<double>(d.Dturns[b], zs);
+                st2(o, b, mk(x.re * p.re - x.im * p.im, x.re * p.im + x.im * p.re));
+            }
+            if (threadIdx.x == 0) {
+                double pk = 0.0;
+                for (int i = 0; i < 7; i++) pk += bi[i] * kp[i];
+                g.pump_save[save_idx] = pp + dt * pk;
+            }
+            save_idx++;
+        }
         z = znew;
 #pragma unroll
         for (int s = 0; s < E; s++) {
@@ -226,14 +270,20 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         dt = fmin(fmax((q == 1.0) ? dt : dt / q, dtmin), L);
     }
 
-    // ---- lab-frame spectrum at the end, pump power and counters
+    // ---- lab-frame spectrum at the end (and the save positions at L), pump
+    // power and counters
 #pragma unroll
     for (int s = 0; s < E; s++) {
         const int b = Sol::bin(s);
         const cx<double> x = ld2(u, b);
         const cx<double> p = phasor<double>(d.Dturns[b], z);
-        st2(d.uL_out, b, mk(x.re * p.re - x.im * p.im, x.re * p.im + x.im * p.re));
+        const cx<double> y = mk(x.re * p.re - x.im * p.im, x.re * p.im + x.im * p.re);
+        st2(d.uL_out, b, y);
+        if (status == ST_OK)
+            for (int si = save_idx; si < d.nsave; si++) st2(d.save_out + (size_t)si * 2 * N, b, y);
     }
+    if (threadIdx.x == 0 && status == ST_OK)
+        for (int si = save_idx; si < d.nsave; si++) g.pump_save[si] = pp;
     if (threadIdx.x == 0) {
         out->naccept = naccept;
         out->nreject = nreject;

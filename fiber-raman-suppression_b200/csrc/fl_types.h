@@ -196,6 +196,7 @@ struct GainDesc {
     const double* sA;       // g_b = sE[b] n2 - sA[b] n1
     const double* sE;
     double pump0;           // P_pump at z = 0 [W]
+    double* pump_save;      // s.nsave pump powers at s.zsave (s.save_out holds the spectra)
 };
 struct GainOut {
     long naccept, nreject, nf;

@@ -113,7 +113,7 @@ def load() -> C.CDLL:
                                           C.POINTER(vp)]
         lib.fl_problem_destroy.argtypes = [vp]
         lib.fl_problem_set_objective.argtypes = [vp, ip, dp]
-        lib.fl_forward_gain.argtypes = [vp, C.POINTER(FlGain), dp, vp, vp, C.POINTER(C.c_double),
+        lib.fl_forward_gain.argtypes = [vp, C.POINTER(FlGain), dp, vp, vp, ip, vp, vp,
                                         C.POINTER(FlStats)]
         lib.fl_forward.argtypes = [vp, vp, vp, ip, vp, C.POINTER(FlStats)]
         lib.fl_adjoint.argtypes = [vp, vp, vp, C.POINTER(FlStats)]
@@ -224,10 +224,11 @@ class GPUProblem:
                                                        float(worst_mode_tau)))
         self.objective = name
 
-    def forward_gain(self, gain, pump_power: float, u0=None):
+    def forward_gain(self, gain, pump_power: float, u0=None, saveat=None):
         """Pump-gain forward solve (fl_forward_gain): gain is a constant gain
-        [1/m] or a fiberlab_gpu.gain.YDFAParams; returns (lab-frame u(L)
-        (1, Nt), pump power at L, stats)."""
+        [1/m] or a fiberlab_gpu.gain.YDFAParams; returns the lab-frame spectra
+        (nsave, 1, Nt) and pump powers (nsave,) at saveat (default [0, L]),
+        and the stats."""
         from . import gain as G
         fp = self.fp
         u0 = np.ascontiguousarray(fp.uw0 if u0 is None else u0, dtype=np.complex128)
@@ -245,12 +246,14 @@ class GPUProblem:
                 arr = np.ascontiguousarray(a[k], dtype=np.float64)
                 keep.append(arr)
                 setattr(g, k, arr.ctypes.data)
-        out = np.empty((1, fp.nt), dtype=np.complex128)
-        pl = C.c_double()
+        z = np.ascontiguousarray([0.0, fp.L] if saveat is None else saveat, dtype=np.float64)
+        out = np.empty((len(z), 1, fp.nt), dtype=np.complex128)
+        pumps = np.empty(len(z))
         st = FlStats()
         self.ctx.check(load().fl_forward_gain(self.h, C.byref(g), float(pump_power), _ptr(u0),
-                                              _ptr(out), C.byref(pl), C.byref(st)))
-        return out, pl.value, st.as_dict()
+                                              _ptr(z), len(z), _ptr(out), _ptr(pumps),
+                                              C.byref(st)))
+        return out, pumps, st.as_dict()
 
     def forward(self, u0=None, saveat=None):
         fp = self.fp

@@ -135,8 +135,11 @@ int fl_problem_set_objective(fl_problem *prob, int objective, double worst_mode_
  * |u_ω|² psd_scale of psd_from_uω, :122-127), whose per-bin arrays are in FFT
  * bin order (the reference's physical-order arrays ifftshift-ed).  M = 1,
  * FP32 mode, Nt = 2^6..2^13; the problem's reltol/abstol apply (the
- * reference fixes reltol = 1e-5).  out_uwL receives the lab-frame spectrum at
- * L (Nt complex), pump_L the pump power there; stats counts the attempts. */
+ * reference fixes reltol = 1e-5).  At each saveat position (sorted, first 0,
+ * last L, as for fl_forward) out_spectra receives the lab-frame spectrum
+ * (Nt complex, position-major) and out_pump the pump power -- the reference's
+ * "uω_z" and "Ppz" (:222-236), from Tsit5's dense interpolant; stats counts
+ * the attempts. */
 #define FL_GAIN_CONSTANT 0
 #define FL_GAIN_YDFA 1
 typedef struct {
@@ -149,7 +152,8 @@ typedef struct {
     const double *sigma_as, *sigma_es, *h_nu_s; /* Nt each, FFT bin order (host memory) */
 } fl_gain;
 int fl_forward_gain(fl_problem *prob, const fl_gain *gain, double pump_power, const double *u0,
-                    double *out_uwL, double *pump_L, fl_stats *stats);
+                    const double *saveat, int nsave, double *out_spectra, double *out_pump,
+                    fl_stats *stats);
 
 /* Forward solve 0 -> L.  Replaces solve_disp_mmf (simulate_disp_mmf.jl:183-207)
  * as used by propagate (propagation.jl:89-123): out_spectra receives the

@@ -930,16 +930,24 @@ int orc_rhs_gain(const orc_problem *p, const orc_gain *g, double z, const orc_c6
 }
 
 int orc_forward_gain(const orc_problem *p, const orc_gain *g, double pump0,
-                     const orc_c64 *u0, orc_c64 *out_uwL, double *pump_L, orc_stats *st) {
+                     const orc_c64 *u0, int nsave, const double *zsave, orc_c64 *out,
+                     double *pump_out, orc_stats *st) {
     gain_ctx c;
     int rc = gain_ctx_init(&c, p, g);
     const int nt = p ? p->nt : 0;
-    cplx *s0 = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * (nt + 1)) : NULL;
-    cplx *sL = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * (nt + 1)) : NULL;
-    if (rc == ORC_OK && (!s0 || !sL)) rc = ORC_ENOMEM;
+    const size_t n = (size_t)nt + 1;
+    if (rc == ORC_OK && (nsave < 0 || (nsave > 0 && (!zsave || !out || !pump_out))))
+        rc = ORC_EINVAL;
+    cplx *s0 = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * n) : NULL;
+    cplx *sL = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * n) : NULL;
+    cplx *sz = rc == ORC_OK ? (cplx *)malloc(sizeof(cplx) * n) : NULL;
+    orc_dense *d = rc == ORC_OK ? (orc_dense *)calloc(1, sizeof(orc_dense)) : NULL;
+    if (rc == ORC_OK && (!s0 || !sL || !sz || !d)) rc = ORC_ENOMEM;
     orc_stats local;
     if (!st) st = &local;
     if (rc == ORC_OK) {
+        d->nt = nt + 1;  /* the dense output of the whole state [P; u~] */
+        d->m = 1;
         /* u0 = vcat(Pp0, u_w0) (simulate_disp_gain_mmf.jl:218-219) */
         s0[0] = pump0;
         for (int b = 0; b < nt; b++) {
@@ -948,21 +956,29 @@ int orc_forward_gain(const orc_problem *p, const orc_gain *g, double pump0,
         }
     }
     if (rc == ORC_OK)
-        rc = tsit5_solve(gain_rhs_cb, &c, (size_t)nt + 1, s0, 0.0, p->L, p->reltol, p->abstol,
-                         sL, st, NULL);
+        rc = tsit5_solve(gain_rhs_cb, &c, n, s0, 0.0, p->L, p->reltol, p->abstol, sL, st, d);
     if (rc == ORC_OK && st->z_end != p->L) rc = ORC_EINVAL;
-    if (rc == ORC_OK) {
-        if (pump_L) *pump_L = creal(sL[0]);
-        if (out_uwL)
-            for (int b = 0; b < nt; b++) {
-                const double a = p->D[b] * p->L;
-                const cplx y = (cos(a) + I * sin(a)) * sL[1 + b];
-                out_uwL[b].re = creal(y);
-                out_uwL[b].im = cimag(y);
-            }
+    for (int k = 0; rc == ORC_OK && k < nsave; k++) {
+        const double z = zsave[k];
+        if (!(z >= 0.0 && z <= p->L)) {
+            rc = ORC_EINVAL;
+            break;
+        }
+        if (z == 0.0) memcpy(sz, s0, sizeof(cplx) * n);
+        else if (z == p->L) memcpy(sz, sL, sizeof(cplx) * n);
+        else orc_dense_eval(d, z, (orc_c64 *)sz);
+        pump_out[k] = creal(sz[0]);
+        for (int b = 0; b < nt; b++) {
+            const double a = p->D[b] * z;
+            const cplx y = (cos(a) + I * sin(a)) * sz[1 + b];
+            out[(size_t)k * nt + b].re = creal(y);
+            out[(size_t)k * nt + b].im = cimag(y);
+        }
     }
     free(s0);
     free(sL);
+    free(sz);
+    orc_dense_free(d);
     gain_ctx_free(&c);
     return rc;
 }

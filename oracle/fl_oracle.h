@@ -108,10 +108,12 @@ int orc_rhs_gain(const orc_problem *p, const orc_gain *g, double z, const orc_c6
 
 /* Pump-gain Tsit5 solve 0 -> L (solve_disp_gain_smf,
  * simulate_disp_gain_mmf.jl:204-239; the reference fixes reltol = 1e-5 and
- * keeps the default abstol: set them in p).  out_uwL receives the lab-frame
- * spectrum at L, pump_L the pump power there. */
+ * keeps the default abstol: set them in p).  At each zsave position (sorted,
+ * within [0, L]) out receives the lab-frame spectrum (Nt complex,
+ * position-major) and pump_out the pump power, from the dense output. */
 int orc_forward_gain(const orc_problem *p, const orc_gain *g, double pump0,
-                     const orc_c64 *u0, orc_c64 *out_uwL, double *pump_L, orc_stats *st);
+                     const orc_c64 *u0, int nsave, const double *zsave, orc_c64 *out,
+                     double *pump_out, orc_stats *st);
 
 /* Fixed-step RK4 scalar restatement (scalar_crosscheck.jl:38-67). */
 int orc_rk4_scalar(const orc_problem *p, const orc_c64 *u0, int steps,

@@ -244,19 +244,21 @@ def rhs_gain(fp, gain, z, pump, u):
     return out[0], out[1:].reshape(1, -1)
 
 
-def forward_gain(fp, gain, pump0, u0=None):
-    """Pump-gain solve 0 -> L (orc_forward_gain): (lab-frame u(L) (1, Nt),
-    pump power at L, stats)."""
+def forward_gain(fp, gain, pump0, u0=None, zsave=None):
+    """Pump-gain solve 0 -> L (orc_forward_gain): lab-frame spectra at zsave
+    ((nsave, 1, Nt); default [0, L]), the pump powers there, and stats."""
     pr = Problem(fp)
     g, keep = _gain_struct(gain)
     u0 = _c(fp.uw0 if u0 is None else u0)
-    out = np.empty(fp.nt, np.complex128)
-    pl = C.c_double()
+    zs = np.ascontiguousarray([0.0, fp.L] if zsave is None else zsave, dtype=np.float64)
+    out = np.empty((len(zs), 1, fp.nt), np.complex128)
+    pumps = np.empty(len(zs))
     st = OrcStats()
     rc = lib().orc_forward_gain(C.byref(pr.s), C.byref(g), C.c_double(pump0),
-                                C.c_void_p(u0.ctypes.data), C.c_void_p(out.ctypes.data),
-                                C.byref(pl), C.byref(st))
+                                C.c_void_p(u0.ctypes.data), len(zs), C.c_void_p(zs.ctypes.data),
+                                C.c_void_p(out.ctypes.data), C.c_void_p(pumps.ctypes.data),
+                                C.byref(st))
     if rc:
         raise OracleError(rc)
-    return out.reshape(1, -1), pl.value, {"naccept": st.naccept, "nreject": st.nreject,
-                                          "nf": st.nf, "z_end": st.z_end}
+    return out, pumps, {"naccept": st.naccept, "nreject": st.nreject, "nf": st.nf,
+                        "z_end": st.z_end}

@@ -55,8 +55,9 @@ def test_ydfa_initialisation_and_pumped_propagation(sections):
     p = G.ydfa_params(fp.sim, ab, em)
     for s in (p.sigma_as, p.sigma_es):
         assert len(s) == fp.nt and np.all(np.isfinite(s)) and np.all(s >= 0)
-    uL, pump_L, st = O.forward_gain(fp, p, 0.05)
-    assert st["z_end"] == fp.L and np.all(np.isfinite(uL)) and np.isfinite(pump_L)
+    out, pumps, st = O.forward_gain(fp, p, 0.05)
+    assert st["z_end"] == fp.L and np.all(np.isfinite(out[-1])) and np.isfinite(pumps[-1])
+    assert pumps[0] == 0.05 and np.array_equal(out[0], fp.uw0)
 
 
 def test_constant_gain_closed_form():
@@ -65,9 +66,12 @@ def test_constant_gain_closed_form():
     fp = P.single_mode_problem(nt=64, time_window_ps=3.0, L=0.5, power_w=1e-3, rep_rate_hz=80e6,
                                gamma=0.0, betas=(0.0,), beta_order=2, fR=0.0, reltol=1e-10,
                                abstol=1e-12)
-    uL, pump_L, _ = O.forward_gain(fp, 0.8, 0.05)
-    assert np.linalg.norm(uL - fp.uw0 * math.exp(0.4 * fp.L)) <= 1e-12 * np.linalg.norm(uL)
-    assert pump_L == pytest.approx(0.05 * math.exp(-fp.L), rel=1e-9)
+    zs = [0.0, 0.17, 0.31, fp.L]
+    out, pumps, _ = O.forward_gain(fp, 0.8, 0.05, zsave=zs)
+    for z, u, pz in zip(zs, out, pumps):
+        # the dense output at interior positions holds to the interpolant's order
+        assert np.linalg.norm(u - fp.uw0 * math.exp(0.4 * z)) <= 1e-9 * np.linalg.norm(u)
+        assert pz == pytest.approx(0.05 * math.exp(-z), rel=1e-9)
 
 
 def test_gain_rhs_matches_literal_restatement():

@@ -483,11 +483,13 @@ def test_gain_propagation_matches_oracle(gpu_ctx, model):
     fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.05,
                                rep_rate_hz=80e6, wavelength_m=1030e-9)
     gain = 0.8 if model == "constant" else G.ydfa_params(fp.sim, *_synthetic_yb_sections())
-    out, pump_L, st = GPUProblem(gpu_ctx, fp).forward_gain(gain, 0.05)
-    ref, pump_ref, rst = O.forward_gain(fp, gain, 0.05)
+    zs = [0.0, 0.1, 0.25, fp.L]
+    out, pumps, st = GPUProblem(gpu_ctx, fp).forward_gain(gain, 0.05, saveat=zs)
+    ref, pumps_ref, rst = O.forward_gain(fp, gain, 0.05, zsave=zs)
     assert st["status"] == 0 and st["z_end"] == fp.L
-    assert rel(out, ref) < FIELD_TOL_FP32
-    assert pump_L == pytest.approx(pump_ref, rel=1e-6)
+    for i in range(len(zs)):
+        assert rel(out[i], ref[i]) < FIELD_TOL_FP32
+        assert pumps[i] == pytest.approx(pumps_ref[i], rel=1e-6)
     assert st["nf"] == 3 + 6 * (st["naccept"] + st["nreject"])
     assert abs(st["naccept"] - rst["naccept"]) <= 2
 
@@ -502,10 +504,13 @@ def test_gain_reference_shape_and_limits(gpu_ctx):
                                wavelength_m=1030e-9, pulse="gauss", reltol=1e-5)
     gain = G.ydfa_params(fp.sim, *_synthetic_yb_sections())
     gp = GPUProblem(gpu_ctx, fp)
-    out, pump_L, st = gp.forward_gain(gain, 0.05)
-    ref, pump_ref, _ = O.forward_gain(fp, gain, 0.05)
-    assert st["status"] == 0 and np.all(np.isfinite(out)) and np.isfinite(pump_L)
-    assert rel(out, ref) < FIELD_TOL_FP32
+    out, pumps, st = gp.forward_gain(gain, 0.05)
+    ref, pumps_ref, _ = O.forward_gain(fp, gain, 0.05)
+    assert st["status"] == 0 and np.all(np.isfinite(out)) and np.all(np.isfinite(pumps))
+    assert rel(out[-1], ref[-1]) < FIELD_TOL_FP32
+    with pytest.raises(FiberLabGPUError) as e:
+        gp.forward_gain(gain, 0.05, saveat=[0.0, 0.5e-5])      # must end at L
+    assert e.value.status == 1
     # built for M = 1, FP32 mode, Nt <= 2^13
     with pytest.raises(FiberLabGPUError) as e:
         GPUProblem(gpu_ctx, fp, "fp64").forward_gain(0.5, 0.05)
