@@ -222,9 +222,11 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
         naccept++;
         double znew = z + dt;
         if (fabs(znew - L) < 100.0 * kEps * fmax(z, L)) znew = L;  // snap to the tstop
-        // save positions in (z, znew]: Tsit5's free interpolant
-        // u_n + dt Σ_i b_i(θ) k_i for the field and the pump power
-        while (save_idx < d.nsave && d.zsave[save_idx] <= znew && d.zsave[save_idx] > z) {
+        // save positions in (z, znew) and on an interior step end: Tsit5's
+        // free interpolant u_n + dt Σ_i b_i(θ) k_i for the field and the pump
+        // power (positions at L take the final state below)
+        while (save_idx < d.nsave && d.zsave[save_idx] > z &&
+               (d.zsave[save_idx] < znew || (d.zsave[save_idx] == znew && znew < L))) {
             const double zs = d.zsave[save_idx], th = (zs - z) / dt;
             double bi[7];
             for (int i = 0; i < 7; i++) {

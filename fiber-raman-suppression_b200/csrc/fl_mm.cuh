@@ -824,8 +824,11 @@ struct MmCtl {
             }
             double znew = z + dt;
             if (fabs(znew - d.L) < 100.0 * kEps * fmax(z, d.L)) znew = d.L;
-            while (st.save_idx < d.nsave && d.zsave[st.save_idx] < znew &&
-                   d.zsave[st.save_idx] > z) {
+            // save positions in (z, znew) and on an interior step end (those
+            // at L take the final state)
+            while (st.save_idx < d.nsave && d.zsave[st.save_idx] > z &&
+                   (d.zsave[st.save_idx] < znew ||
+                    (d.zsave[st.save_idx] == znew && znew < d.L))) {
                 const double zs = d.zsave[st.save_idx];
                 const double th = (zs - z) / dt;
                 double bi[7];

@@ -1031,9 +1031,10 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             }
             double znew = z + dt;
             if (fabs(znew - L) < 100.0 * kEps * fmax(z, L)) znew = L;  // snap to the tstop
-            // save positions strictly inside (z, znew): dense output
-            while (st.save_idx < d.nsave && d.zsave[st.save_idx] < znew &&
-                   d.zsave[st.save_idx] > z) {
+            // save positions in (z, znew) and on an interior step end: dense
+            // output (positions at L take the final state below)
+            while (st.save_idx < d.nsave && d.zsave[st.save_idx] > z &&
+                   (d.zsave[st.save_idx] < znew || (d.zsave[st.save_idx] == znew && znew < L))) {
                 const double zs = d.zsave[st.save_idx];
                 const double th = (zs - z) / dt;
                 double* o = d.save_out + (size_t)st.save_idx * 2 * N;
