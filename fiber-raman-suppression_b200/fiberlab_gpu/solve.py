@@ -5,6 +5,7 @@ error behaviour:
 
   solve_disp_mmf(uω0, fiber, sim)            src/simulation/simulate_disp_mmf.jl:183-207
   solve_adjoint_disp_mmf(λωL, ũω, fiber, sim) src/simulation/sensitivity_disp_mmf.jl:309-332
+  solve_disp_gain_smf(uω0, fiber, sim)       src/simulation/simulate_disp_gain_mmf.jl:204-239
   propagate(problem; saveat)                 src/fiberlab/propagation.jl:89-123
   metrics(result), verify(result; ...)       src/fiberlab/propagation.jl:176-304
   physical phase gradient                    src/fiberlab/physics_models.jl:1033-1046
@@ -132,6 +133,39 @@ def solve_adjoint_disp_mmf(lamL, sol: GPUSolution, fiber: dict, sim: dict) -> GP
     L = float(fiber["L"])
     return GPUSolution(sol._gp, [0.0, L], np.stack([lam0, np.exp(-1j * np.asarray(fiber["Dω"]) * L) * lam]),
                        stats, frame="adjoint")
+
+
+def solve_disp_gain_smf(uw0, fiber: dict, sim: dict, *, pump_power: float = 0.0,
+                        ctx: Context = None) -> dict:
+    """solve_disp_gain_smf (simulate_disp_gain_mmf.jl:204-239) on the GPU
+    (fl_forward_gain).  Single mode only; fiber["gain_parameters"] is a
+    constant gain [1/m] or a gain.YDFAParams (default 0.0, :210); the solve
+    uses the reference's reltol = 1e-5 with the default abstol (:214-216).
+    Returns {"ode_sol": GPUSolution} (its `pump` holds P at the stored
+    positions) and, when fiber["zsave"] is set, the lab-frame "uω_z"
+    (Nz, 1, Nt), "ut_z" (fft along time) and "Ppz" (Nz, 1) (:222-236)."""
+    if int(sim.get("M", 0)) != 1:
+        raise P.ArgumentError("disp_gain_smf is single mode only, requires M = 1 "
+                              f"(got M = {sim.get('M')})")
+    gain = fiber.get("gain_parameters", 0.0)
+    fp = problem_from_dicts(uw0, fiber, sim)
+    fp.reltol, fp.abstol = 1e-5, 1e-6
+    zsave = fiber.get("zsave")
+    zs = [0.0, fp.L]
+    if zsave is not None:
+        zs = sorted(set(zs + [float(z) for z in zsave]))
+    gp = GPUProblem(ctx or default_context(), fp)
+    lab, pumps, stats = gp.forward_gain(gain, float(pump_power), fp.uw0, zs)
+    inter = np.stack([np.exp(-1j * fp.D * z) * lab[i] for i, z in enumerate(zs)])
+    sol = GPUSolution(gp, zs, inter, stats)
+    sol.pump = np.asarray(pumps)
+    out = {"ode_sol": sol}
+    if zsave is not None:
+        sel = [zs.index(float(z)) for z in zsave]
+        out["uω_z"] = lab[sel]
+        out["ut_z"] = np.fft.fft(lab[sel], axis=-1)
+        out["Ppz"] = np.asarray(pumps)[sel][:, None]
+    return out
 
 
 @dataclass

@@ -84,3 +84,44 @@ def test_adjoint_terminal_condition_checks(fp):
     g[0, 0, 1, 1] = 1.0
     with pytest.raises(P.ArgumentError, match="symmetric"):
         S.solve_adjoint_disp_mmf(fp.uw0, None, dict(fiber, **{"γ": g}), sim)
+
+
+def test_solve_disp_gain_smf_assembly(monkeypatch):
+    # the dictionary interface and output assembly of solve_disp_gain_smf
+    # (simulate_disp_gain_mmf.jl:204-239) around a stand-in for the device
+    # call that returns the closed form of a constant gain with no
+    # nonlinearity or dispersion (the GPU path itself is checked in
+    # tests/test_gpu_parity.py::test_gain_propagation_matches_oracle)
+    seen = {}
+
+    class ClosedForm:
+        def __init__(self, ctx, fp, precision="fp32"):
+            self.fp = fp
+            seen["tol"] = (fp.reltol, fp.abstol)
+
+        def forward_gain(self, gain, pump, u0, saveat):
+            z = np.asarray(saveat)
+            out = np.stack([u0 * np.exp(0.5 * gain * zz) for zz in z])
+            return out, pump * np.exp(-z), {"naccept": 3, "nreject": 0, "nf": 21,
+                                            "adj_naccept": 0, "adj_nreject": 0, "adj_nf": 0}
+    monkeypatch.setattr(S, "GPUProblem", ClosedForm)
+    monkeypatch.setattr(S, "default_context", lambda: None)
+    fp = P.single_mode_problem(nt=64, time_window_ps=3.0, L=0.2, power_w=1e-3, rep_rate_hz=80e6,
+                               gamma=0.0, betas=(0.0,), beta_order=2, fR=0.0)
+    fiber, sim = _dicts(fp)
+    fiber["gain_parameters"] = 0.6
+    fiber["zsave"] = [0.05, 0.2]
+    res = S.solve_disp_gain_smf(fp.uw0, fiber, sim, pump_power=0.05)
+    assert seen["tol"] == (1e-5, 1e-6)       # the reference's fixed reltol, default abstol
+    assert res["uω_z"].shape == (2, 1, fp.nt) and res["Ppz"].shape == (2, 1)
+    assert np.allclose(res["uω_z"][1], fp.uw0 * np.exp(0.3 * 0.2), rtol=1e-14)
+    assert np.allclose(res["Ppz"][:, 0], 0.05 * np.exp(-np.array([0.05, 0.2])), rtol=1e-14)
+    assert np.array_equal(res["ut_z"], np.fft.fft(res["uω_z"], axis=-1))
+    sol = res["ode_sol"]
+    assert list(sol.t) == [0.0, 0.05, 0.2] and sol.pump[0] == 0.05
+    assert sol.destats.naccept == 3 and sol.retcode == "Success"
+    assert np.allclose(sol(0.2), np.exp(-1j * fp.D * 0.2) * res["uω_z"][1])
+    del fiber["zsave"]
+    assert set(S.solve_disp_gain_smf(fp.uw0, fiber, sim, pump_power=0.05)) == {"ode_sol"}
+    with pytest.raises(P.ArgumentError, match="single mode only"):
+        S.solve_disp_gain_smf(fp.uw0, fiber, dict(sim, M=2))
