@@ -28,7 +28,8 @@ using namespace fl;
 
 struct fl_ctx {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // the stream every call of this context runs on
+    cudaStream_t own = nullptr;     // the context's private stream (the default for stream)
     std::string err;
     fl_ctx_opts opts{};
     long launches = 0;
@@ -184,6 +185,14 @@ struct Work {
 
 namespace {
 
+// Accepted-step log entries per slot: the option, or (0) one per attempted
+// step allowed, so the log never limits a solve that the attempted-step
+// limit admits.
+int step_log_entries(const fl_ctx_opts& o) {
+    if (o.step_log > 0) return o.step_log;
+    return (int)std::min<long>(o.max_iters, 1L << 30);
+}
+
 // rf: bytes of one forward-precision real (4 or 8); the adjoint is FP64
 size_t slot_bytes(int nt, size_t rf, int K, int segcap, int stepcap) {
     const size_t C = 2 * rf * nt, D2 = 16 * (size_t)nt;
@@ -218,7 +227,7 @@ int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out,
     w->rsize = (int)rf;
     w->K = o.checkpoints;
     w->segcap = o.segment_steps;
-    w->stepcap = o.step_log;
+    w->stepcap = step_log_entries(o);
     w->nsave = nsave;
     const int nt = pr->nt;
     const size_t per = slot_bytes(nt, rf, w->K, w->segcap, w->stepcap);
@@ -488,7 +497,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     w->np = pr->m * (pr->m + 1) / 2;
     w->K = o.checkpoints;
     w->segcap = o.segment_steps;
-    w->stepcap = o.step_log;
+    w->stepcap = step_log_entries(o);
     w->nsave = nsave;
     w->per_mode = per_mode;
     const size_t nm = (size_t)pr->nt * pr->m, npn = (size_t)w->np * pr->nt;
@@ -631,15 +640,17 @@ int mm_run(fl_problem* pr, MmWork* w, int nactive) {
     const int per_batch = 8;
     // one batch: 8 evaluation rounds, the counter of finished slots reset
     // before the last round (which counts them)
-    auto enqueue_batch = [&]() -> cudaError_t {
+    auto enqueue_batch = [&](cudaStream_t cs) -> cudaError_t {
+        MmRound b = a;
+        b.stream = cs;
         for (int r = 0; r < per_batch; r++) {
-            a.ndone = nullptr;
+            b.ndone = nullptr;
             if (r == per_batch - 1) {
-                const cudaError_t e = cudaMemsetAsync(w->d_ndone, 0, sizeof(int), ctx->stream);
+                const cudaError_t e = cudaMemsetAsync(w->d_ndone, 0, sizeof(int), cs);
                 if (e != cudaSuccess) return e;
-                a.ndone = w->d_ndone;
+                b.ndone = w->d_ndone;
             }
-            const cudaError_t e = round(a);
+            const cudaError_t e = round(b);
             if (e != cudaSuccess) return e;
         }
         return cudaSuccess;
@@ -648,15 +659,17 @@ int mm_run(fl_problem* pr, MmWork* w, int nactive) {
     // reads every slot's phase from device memory, so the same launches serve
     // every batch, and a batch costs one graph launch instead of 8 x 7..10
     // kernel launches.  Capture is thread-local (other host threads, e.g. a
-    // server's, keep launching).
+    // server's, keep launching) and runs on the context's private stream, so
+    // a caller's stream (which may be the legacy default stream) is never put
+    // in capture mode; the graph is launched on the context's current stream.
     if (!w->graph || w->graph_nactive != nactive) {
         if (w->graph) cudaGraphExecDestroy(w->graph);
         w->graph = nullptr;
         w->graph_nactive = -1;
         cudaGraph_t g = nullptr;
-        CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t e1 = enqueue_batch();
-        const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &g);
+        CU(cudaStreamBeginCapture(ctx->own, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t e1 = enqueue_batch(ctx->own);
+        const cudaError_t e2 = cudaStreamEndCapture(ctx->own, &g);
         if (e1 != cudaSuccess || e2 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
@@ -1000,10 +1013,11 @@ namespace {
 size_t srv_slot_bytes(const fl_server* sv, const fl_problem* pr) {
     const size_t rf = pr->precision == FL_PRECISION_FP64 ? 8 : 4;
     const fl_ctx_opts& o = sv->wopts;
-    if (!pr->use_mm) return slot_bytes(pr->nt, rf, o.checkpoints, o.segment_steps, o.step_log) +
+    if (!pr->use_mm) return slot_bytes(pr->nt, rf, o.checkpoints, o.segment_steps,
+                                       step_log_entries(o)) +
                             16 * (size_t)pr->nt * 4 + 8 * (size_t)pr->nt + 2 * (size_t)pr->nt;
     const size_t nm = (size_t)pr->nt * pr->m, np = (size_t)pr->m * (pr->m + 1) / 2;
-    return mm_slot_bytes(nm, np * pr->nt, rf, o.checkpoints, o.segment_steps, o.step_log,
+    return mm_slot_bytes(nm, np * pr->nt, rf, o.checkpoints, o.segment_steps, step_log_entries(o),
                          pr->m * mm_cluster_ctas(ilog2i(pr->nt))) +
            16 * nm * 4 + 8 * nm + 2 * (size_t)pr->nt;
 }
@@ -1401,7 +1415,7 @@ int fl_ctx_create(int device, const fl_ctx_opts* opts, fl_ctx** out) {
     ctx->opts.hbm_budget_bytes = 0;
     ctx->opts.checkpoints = 32;
     ctx->opts.segment_steps = 16;
-    ctx->opts.step_log = 16384;
+    ctx->opts.step_log = 0;  // one entry per allowed attempted step
     ctx->opts.max_iters = 100000;
     if (opts) {
         if (opts->hbm_budget_bytes) ctx->opts.hbm_budget_bytes = opts->hbm_budget_bytes;
@@ -1411,7 +1425,7 @@ int fl_ctx_create(int device, const fl_ctx_opts* opts, fl_ctx** out) {
         if (opts->max_iters) ctx->opts.max_iters = opts->max_iters;
     }
     if (!pow2(ctx->opts.checkpoints) || ctx->opts.checkpoints < 2 ||
-        ctx->opts.segment_steps < 1 || ctx->opts.step_log < 1 || ctx->opts.max_iters < 1) {
+        ctx->opts.segment_steps < 1 || ctx->opts.step_log < 0 || ctx->opts.max_iters < 1) {
         delete ctx;
         return FL_EINVAL;
     }
@@ -1425,10 +1439,11 @@ int fl_ctx_create(int device, const fl_ctx_opts* opts, fl_ctx** out) {
         return FL_ENODEV;
     }
     ctx->sm_count = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return FL_ECUDA;
     }
+    ctx->stream = ctx->own;
     for (auto& e : ctx->ev)
         if (cudaEventCreate(&e) != cudaSuccess) {
             fl_ctx_destroy(ctx);
@@ -1442,10 +1457,22 @@ int fl_ctx_destroy(fl_ctx* ctx) {
     if (!ctx) return FL_EINVAL;
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return FL_OK;
 }
+
+int fl_ctx_set_stream(fl_ctx* ctx, void* stream) {
+    if (!ctx) return FL_EINVAL;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    // work already queued on the previous stream completes before the switch,
+    // so the context's device buffers are never used by two streams at once
+    CU(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own;
+    return FL_OK;
+}
+
+void* fl_ctx_get_stream(const fl_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 const char* fl_last_error(const fl_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
@@ -1615,13 +1642,17 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
     // one device area: launch, two states, seven FP32 stages, two scratch
     // fields, error partial and weights, output, gain tables, descriptor, result
+    // (the size is the sum of the regions taken below, each rounded up to the
+    // 256-byte alignment that take() gives it)
     const size_t F = 16 * (size_t)nt, H = 8 * (size_t)nt;
-    const size_t bytes = F * 4 + H * 7 + F * 2 + F + H + 4 * H + F * (size_t)nsave +
-                         16 * (size_t)nsave + sizeof(GainDesc) + sizeof(GainOut) + 4 * 256;
+    auto al = [](size_t n) { return (n + 255) & ~size_t(255); };
+    const size_t bytes = 4 * al(F) + 7 * al(H) + 2 * al(F) + al(F) + al(H) + al(4 * H) +
+                         al(8 * (size_t)nsave) + al(F * (size_t)nsave) + al(8 * (size_t)nsave) +
+                         al(sizeof(GainDesc)) + al(sizeof(GainOut));
     char* pool = nullptr;
     CU(cudaMalloc(&pool, bytes));
     char* p = pool;
-    auto take = [&](size_t n) { char* q = p; p += (n + 255) & ~size_t(255); return q; };
+    auto take = [&](size_t n) { char* q = p; p += al(n); return q; };
     GainDesc hd;
     memset(&hd, 0, sizeof hd);
     SlotDesc& d = hd.s;
@@ -1666,6 +1697,11 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
     hd.pump0 = pump_power;
     GainDesc* d_desc = (GainDesc*)take(sizeof(GainDesc));
     GainOut* d_out = (GainOut*)take(sizeof(GainOut));
+    if ((size_t)(p - pool) > bytes) {
+        cudaFree(pool);
+        return set_err(ctx, FL_ECUDA, "internal: gain workspace overflow (%zu > %zu)",
+                       (size_t)(p - pool), bytes);
+    }
     GainOut ho{};
     cudaError_t e = cudaMemcpyAsync(d_u0, u0, F, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
@@ -1785,6 +1821,48 @@ int fl_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats*
     if (stats) fill_stats(st[0], stats);
     if (st[0].status) return set_err(ctx, st[0].status, "%s", fl_status_string(st[0].status));
     CU(cudaMemcpy(lambda0, w->d_lam0, 16 * (size_t)nt, cudaMemcpyDeviceToHost));
+    return FL_OK;
+}
+
+int fl_forward_times(fl_problem* pr, double* t_out, long cap, long* n_out) {
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!n_out || (cap > 0 && !t_out)) return set_err(ctx, FL_EINVAL, "null argument");
+    if (!(pr->use_mm ? (void*)pr->mlast : (void*)pr->last))
+        return set_err(ctx, FL_EINVAL, "fl_forward_times needs a preceding fl_forward");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    // the accepted-step log (z_n, dt_n) of slot 0 and its final position
+    long nsteps = 0;
+    double zend = 0.0;
+    const double* d_log = nullptr;
+    if (pr->use_mm) {
+        std::vector<MmState> st;
+        rc = mm_read_states(ctx, pr->mlast, 1, st);
+        if (rc) return rc;
+        if (st[0].status != ST_OK || st[0].nsteps <= 0)
+            return set_err(ctx, FL_EINVAL, "the last forward did not complete");
+        nsteps = st[0].nsteps;
+        zend = st[0].z;
+        d_log = pr->mlast->h_desc[0].steplog;
+    } else {
+        std::vector<SlotState> st;
+        rc = read_states(ctx, pr->last, st);
+        if (rc) return rc;
+        if (st[0].status != ST_OK || st[0].nsteps <= 0)
+            return set_err(ctx, FL_EINVAL, "the last forward did not complete");
+        nsteps = st[0].nsteps;
+        zend = st[0].z;
+        d_log = reinterpret_cast<const SlotDesc*>(pr->last->h_desc.data())[0].steplog;
+    }
+    *n_out = nsteps + 1;
+    if (cap <= 0) return FL_OK;
+    std::vector<double> lg(2 * (size_t)nsteps);
+    CU(cudaMemcpyAsync(lg.data(), d_log, sizeof(double) * lg.size(), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (long i = 0; i < nsteps && i < cap; i++) t_out[i] = lg[2 * i];
+    if (nsteps < cap) t_out[nsteps] = zend;
     return FL_OK;
 }
 
@@ -2003,8 +2081,7 @@ int fl_server_create(fl_ctx* ctx, const fl_server_opts* opts, fl_server** out) {
     sv->wopts = ctx->opts;
     sv->wopts.checkpoints = sv->opts.checkpoints;
     sv->wopts.segment_steps = sv->opts.segment_steps;
-    sv->wopts.step_log = std::max(ctx->opts.step_log,
-                                  sv->opts.checkpoints * sv->opts.segment_steps);
+    sv->wopts.step_log = 0;  // one entry per allowed attempted step
     sv->wopts.max_iters = std::max(ctx->opts.max_iters, 400000L);
     fl_server* p = sv.release();
     p->th = std::thread(srv_thread, p);

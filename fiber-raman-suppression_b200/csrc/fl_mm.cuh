@@ -245,12 +245,12 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.lamL, off + tid + TT * s));
     } else {
-        const int seg_lo = st.seg * st.ck_stride;
-        const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
+        const SubSeg sb = sub_segment(d, st);
+        const int seg_lo = sb.lo;
         const double zz = st.ezload;
         const double* lg = d.steplog;
         // last stored step starting at or before zz, by bisection
-        int n = seg_lo, hi = seg_hi - 1;
+        int n = seg_lo, hi = sb.hi - 1;
         while (n < hi) {
             const int mid = (n + hi + 1) >> 1;
             if (lg[2 * mid] <= zz) n = mid;
@@ -417,10 +417,13 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     else dst = static_cast<C*>(mm_kp(d.kf, st.kperm, st.stage));
 #pragma unroll
     for (int s = 0; s < E; s++) dst[off + tid + TT * s] = v[s];
-    if (st.stage == 6 && ph == PH_REC) {
+    const SubSeg sb = sub_segment(d, st);
+    if (st.stage == 6 && ph == PH_REC && sb.seg_lo + st.rec_pos >= sb.lo) {
         // dense interpolant of the replayed step, this mode's part:
-        // c0 = ũ_n, c_p = Σ_i r_ip k_i (Tsit5's free 4th-order interpolant)
-        const size_t NM = (size_t)N * d.M, base = (size_t)st.rec_pos * 5 * NM;
+        // c0 = ũ_n, c_p = Σ_i r_ip k_i (Tsit5's free 4th-order interpolant),
+        // kept for the steps of the current sub-segment only
+        const size_t NM = (size_t)N * d.M,
+                     base = (size_t)(sb.seg_lo + st.rec_pos - sb.lo) * 5 * NM;
         C* sg = static_cast<C*>(d.seg);
         const double* un = d.u[st.cur];
 #pragma unroll 1
@@ -789,9 +792,8 @@ struct MmCtl {
                 st.cur ^= 1;
                 st.kperm ^= 1;
                 st.rec_pos++;
-                const int seg_lo = st.seg * st.ck_stride;
-                if (seg_lo + st.rec_pos >= min(seg_lo + st.ck_stride, st.nsteps))
-                    st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
+                const SubSeg sb = sub_segment(d, st);
+                if (sb.seg_lo + st.rec_pos >= sb.hi) st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
                 return;
             }
             double acc = 0.0;
@@ -894,7 +896,7 @@ struct MmCtl {
             }
             st.stage = 0;
             const double z = st.cz, dt = st.cdt;
-            const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
+            const double zlo = d.steplog[2 * sub_segment(d, st).lo];
             double acc = 0.0;
             for (int m = 0; m < d.nparts; m++) acc += d.part[m];
             const double EEst = sqrt(acc / (double)NM);
@@ -923,10 +925,16 @@ struct MmCtl {
             if (adt < st.aprop) dtn = fmax(dtn, st.aprop);  // shortened for a segment start
             st.adt = -dtn;
             if (st.az == zlo) {
-                if (st.seg == 0) {
+                if (st.sub > 0) {  // the previous sub-segment of this segment
+                    st.sub--;
+                    __syncthreads();
+                    restore_checkpoint(st.seg);
+                    st.phase = PH_REC;
+                } else if (st.seg == 0) {
                     st.phase = PH_FINAL;
                 } else {
                     st.seg--;
+                    st.sub = last_sub(d, st, st.seg);
                     __syncthreads();
                     restore_checkpoint(st.seg);
                     st.phase = PH_REC;
@@ -1007,7 +1015,7 @@ struct MmCtl {
             }
             if (ph == PH_ADJ_INIT) {
                 st.ez = st.stage == 0 ? L : L - st.cdt;
-                st.ezload = st.stage == 0 ? L : fmax(st.ez, d.steplog[2 * (st.seg * st.ck_stride)]);
+                st.ezload = st.stage == 0 ? L : fmax(st.ez, d.steplog[2 * sub_segment(d, st).lo]);
                 return;
             }
             // PH_ADJ
@@ -1019,7 +1027,7 @@ struct MmCtl {
                 }
                 // segment starts are made transparent to the controller (no
                 // sliver step before one; the pre-clip proposal is restored)
-                const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
+                const double zlo = d.steplog[2 * sub_segment(d, st).lo];
                 const double prop = fmax(fmin(fabs(st.adt), L), dtmin);
                 const double rem = st.az - zlo;
                 double adt = prop;
@@ -1154,12 +1162,8 @@ struct MmCtl {
             return;
         }
         st.abstol_adj = scl == 0.0 ? d.abstol : d.abstol * scl;  // sensitivity_disp_mmf.jl:324-325
-        if (st.ck_stride > d.seg_cap) {
-            st.status = ST_CAPACITY;
-            st.phase = PH_DONE;
-            return;
-        }
         st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
+        st.sub = last_sub(d, st, st.seg);
         st.acur = 0;
         st.akperm = 0;
         st.a_naccept = st.a_nreject = st.a_nf = st.a_iters = 0;

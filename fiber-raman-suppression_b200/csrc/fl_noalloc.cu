@@ -23,11 +23,11 @@ namespace {
 
 // Scratch budget: descriptor, state and tables plus the FP32 forward
 // workspace (two FP64 states, seven FP32 stages, scratch fields, the error
-// buffers) and a step log of FL_NOALLOC_MAX_STEPS entries.
+// buffers).  A forward-only solve keeps no step log and no checkpoints, so
+// the number of steps is not limited by the scratch size.
 constexpr size_t kScratchBytes = 2u << 20;  // 2 MiB per device
 constexpr int kMaxLogN = 13;                // Nt <= 2^13
 constexpr int kMinLogN = 6;
-constexpr int kMaxSteps = 8192;             // accepted forward steps
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -38,8 +38,7 @@ size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Offsets of every region inside the scratch array for nt points.
 struct Layout {
-    size_t desc, state, active, dturns, heff, ss, tw, u0b, u1b, kf[7], scr0, scr1, esv, skv,
-        steplog, end;
+    size_t desc, state, active, dturns, heff, ss, tw, u0b, u1b, kf[7], scr0, scr1, esv, skv, end;
     explicit Layout(int nt) {
         size_t p = 0;
         auto take = [&](size_t bytes) {
@@ -61,7 +60,6 @@ struct Layout {
         scr1 = take(16 * (size_t)nt);
         esv = take(16 * (size_t)nt);
         skv = take(8 * (size_t)nt);
-        steplog = take(16 * (size_t)kMaxSteps);
         end = p;
     }
 };
@@ -103,6 +101,21 @@ __global__ void noalloc_prepare(SlotDesc desc, unsigned char* base, Layout lay, 
     }
 }
 
+// Restores the calling thread's current device on every return path: the
+// callers of this entry point (host runtimes that own the device) must not
+// find their thread moved to another device.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) return;
+        ok = prev == device || cudaSetDevice(device) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (ok && prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" int fl_forward_noalloc(int device, int nt, const double* d_D, double gamma,
@@ -122,7 +135,11 @@ extern "C" int fl_forward_noalloc(int device, int nt, const double* d_D, double 
     if (device < 0 || device >= kMaxDevices) return FL_ENODEV;
     const Layout lay(nt);
     if (lay.end > kScratchBytes) return FL_EUNSUPPORTED;
-    if (cudaSetDevice(device) != cudaSuccess) return FL_ENODEV;
+    DeviceGuard guard(device);
+    if (!guard.ok) return FL_ENODEV;
+    // an error left pending by earlier work on this thread is not this
+    // call's: report it without consuming it
+    if (cudaPeekAtLastError() != cudaSuccess) return FL_ECUDA;
     // one-time set-up per device (with that device current): the device
     // address of the scratch array; the host-side symbol is not a device address
     if (!g_scratch_addr[device]) {
@@ -145,9 +162,9 @@ extern "C" int fl_forward_noalloc(int device, int nt, const double* d_D, double 
     d.abstol = abstol;
     d.mode = MODE_FORWARD;
     d.nsave = nsave;
-    d.ck_cap = 0;  // forward only: no z-checkpoints
+    d.ck_cap = 0;    // forward only: no z-checkpoints,
     d.seg_cap = 0;
-    d.step_cap = kMaxSteps;
+    d.step_cap = 0;  // no step log (nothing is kept for an adjoint)
     d.max_iters = 100000;
     d.zsave = d_saveat;
     d.save_out = d_out_spectra;
@@ -159,10 +176,9 @@ extern "C" int fl_forward_noalloc(int device, int nt, const double* d_D, double 
     d.scr[1] = base + lay.scr1;
     d.esv = reinterpret_cast<double*>(base + lay.esv);
     d.skv = reinterpret_cast<double*>(base + lay.skv);
-    d.steplog = reinterpret_cast<double*>(base + lay.steplog);
 
     noalloc_prepare<<<(nt + 255) / 256, 256, 0, s>>>(d, base, lay, nt, d_D, d_hR, d_selfsteep);
-    if (cudaGetLastError() != cudaSuccess) return FL_ECUDA;
+    if (cudaGetLastError() != cudaSuccess) return FL_ECUDA;  // this launch's own error
     LaunchFn fn = sm_launcher(0, logn);
     if (!fn) return FL_EUNSUPPORTED;
     LaunchArgs a{base + lay.desc, reinterpret_cast<SlotState*>(base + lay.state),

@@ -555,6 +555,34 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     }
 }
 
+// Steps [lo, hi) of the current sub-segment: the segment of checkpoint seg
+// (ck_stride steps) is replayed and integrated backward in sub-segments of at
+// most seg_cap steps, last first.  Each sub-segment replays the segment from
+// its checkpoint; the steps before the sub-segment are recomputed without
+// storing their interpolant, so a solve of any length fits the K checkpoints
+// and the seg_cap-step interpolant buffer (at the cost of recomputation that
+// grows with ck_stride / seg_cap) instead of failing for capacity.
+// (Shared by the single-mode and the multimode steppers: Desc / State are
+// SlotDesc / SlotState or MmDesc / MmState.)
+struct SubSeg {
+    int seg_lo, seg_hi, lo, hi;
+};
+template <class Desc, class State>
+__device__ __forceinline__ SubSeg sub_segment(const Desc& d, const State& st) {
+    SubSeg r;
+    r.seg_lo = st.seg * st.ck_stride;
+    r.seg_hi = min(r.seg_lo + st.ck_stride, st.nsteps);
+    r.lo = r.seg_lo + st.sub * d.seg_cap;
+    r.hi = min(r.lo + d.seg_cap, r.seg_hi);
+    return r;
+}
+// index of the last sub-segment of segment seg
+template <class Desc, class State>
+__device__ __forceinline__ int last_sub(const Desc& d, const State& st, int seg) {
+    const int lo = seg * st.ck_stride, hi = min(lo + st.ck_stride, st.nsteps);
+    return (hi - lo - 1) / d.seg_cap;
+}
+
 template <typename RF, int LOGN, int LOGE>
 __device__ __forceinline__ void restore_checkpoint(const SlotDesc& d, int seg, SlotState& st) {
     using S = FftShape<LOGN, LOGE>;
@@ -738,12 +766,8 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 continue;
             }
             st.abstol_adj = scl == 0.0 ? d.abstol : d.abstol * scl;  // sensitivity_disp_mmf.jl:324-325
-            if (st.ck_stride > d.seg_cap) {
-                st.status = ST_CAPACITY;
-                st.phase = PH_DONE;
-                continue;
-            }
             st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
+            st.sub = last_sub(d, st, st.seg);
             st.acur = 0;
             st.akperm = 0;
             st.a_naccept = st.a_nreject = st.a_nf = st.a_iters = 0;
@@ -836,9 +860,9 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 }
             }
             ze = st.stage == 0 ? L : L - st.cdt;
-            zload = st.stage == 0 ? L : fmax(ze, d.steplog[2 * (st.seg * st.ck_stride)]);
+            zload = st.stage == 0 ? L : fmax(ze, d.steplog[2 * sub_segment(d, st).lo]);
         } else {  // PH_ADJ
-            const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
+            const double zlo = d.steplog[2 * sub_segment(d, st).lo];
             if (st.stage == 0) {
                 if (++st.a_iters > d.max_iters) {
                     st.status = ST_MAXITERS;
@@ -871,9 +895,8 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 
         // ------------------------------------------------ one RHS evaluation
         if (adj) {
-            const int seg_lo = st.seg * st.ck_stride;
-            const int seg_hi = min(seg_lo + st.ck_stride, st.nsteps);
-            rhs_adj_call<RF, RA, LOGN, LOGE>(&d, smraw, red, ze, va, seg_lo, seg_hi, zload,
+            const SubSeg sb = sub_segment(d, st);
+            rhs_adj_call<RF, RA, LOGN, LOGE>(&d, smraw, red, ze, va, sb.lo, sb.hi, zload,
                                              nullptr);
         } else {
             rhs_fwd_call<RF, LOGN, LOGE>(&d, smraw, red, ze, vf);
@@ -961,10 +984,14 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double* u = d.u[st.cur];
             if (rec) {
                 // interpolant of this step: c0 = ũ_n, c_p = Σ_i r_ip k_i
-                // (stage-outer over chunks of 4 points, as in stage_input)
-                CF* sg = (CF*)d.seg + (size_t)st.rec_pos * 5 * N;
+                // (stage-outer over chunks of 4 points, as in stage_input),
+                // kept only for the steps of the current sub-segment
+                const SubSeg sb = sub_segment(d, st);
+                const int n = sb.seg_lo + st.rec_pos;
+                CF* sg = (CF*)d.seg + (size_t)max(n - sb.lo, 0) * 5 * N;
                 constexpr int RC = E < 4 ? E : 4;
                 static_assert(E % RC == 0, "chunks tile the thread's points");
+                if (n >= sb.lo)
 #pragma unroll
                 for (int s0 = 0; s0 < E; s0 += RC) {
                     double cr[RC][4], ci[RC][4];
@@ -998,9 +1025,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 st.cur ^= 1;
                 st.kperm ^= 1;
                 st.rec_pos++;
-                const int seg_lo = st.seg * st.ck_stride;
-                if (seg_lo + st.rec_pos >= min(seg_lo + st.ck_stride, st.nsteps))
-                    st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
+                if (n + 1 >= sb.hi) st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
                 continue;
             }
             const double EEst = SF.error_norm(vf, dt);
@@ -1121,7 +1146,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             }
             st.stage = 0;
             const double z = st.cz, dt = st.cdt;
-            const double zlo = d.steplog[2 * (st.seg * st.ck_stride)];
+            const double zlo = d.steplog[2 * sub_segment(d, st).lo];
             const double EEst = SA.error_norm(va, dt);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;
@@ -1148,10 +1173,15 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             if (adt < st.aprop) dtn = fmax(dtn, st.aprop);  // shortened for a segment start
             st.adt = -dtn;
             if (st.az == zlo) {
-                if (st.seg == 0) {
+                if (st.sub > 0) {  // the previous sub-segment of this segment
+                    st.sub--;
+                    restore_checkpoint<RF, LOGN, LOGE>(d, st.seg, st);
+                    st.phase = PH_REC;
+                } else if (st.seg == 0) {
                     st.phase = PH_FINAL;
                 } else {
                     st.seg--;
+                    st.sub = last_sub(d, st, st.seg);
                     restore_checkpoint<RF, LOGN, LOGE>(d, st.seg, st);
                     st.phase = PH_REC;
                 }

@@ -147,6 +147,7 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
     cx<float>* eta = static_cast<cx<float>*>(d.eta);
     uint32_t phase = 0;
     bool ok = true;
+    int mma_pending = -1;  // parity of a commit whose arrival a timed-out wait did not see
     for (int tile = first; tile < ntiles; tile += step) {
         const int t = tile * kTcRows + tid;
         if (!ok) {  // an earlier tile timed out: no more MMAs from this CTA
@@ -233,6 +234,7 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
                 : "r"(smem_u32(mbar)), "r"(phase)
                 : "memory");
         }
+        if (!done && mma_pending < 0) mma_pending = (int)phase;
         phase ^= 1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         ok = ok && done;
@@ -256,9 +258,12 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
             }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         }
-        // the next tile's MMAs overwrite the accumulator and A: all reads done first
+        // the next tile's MMAs overwrite the accumulator and A: all reads done
+        // first.  The barrier also makes ok block-uniform (a wait that gave up
+        // in any thread stops the CTA's MMAs), so every thread takes the same
+        // path through the remaining tiles and their barriers.
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
+        ok = __syncthreads_and(ok ? 1 : 0) != 0;
         ok = ok && !*bfail;
 
         // ---- η_i = Σ_j δ_ij u_j
@@ -287,6 +292,24 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
                 "selp.u32 %0, 1, 0, p;\n\t}\n"
                 : "=r"(got)
                 : "r"(smem_u32(bbar))
+                : "memory");
+        }
+    }
+    // ---- MMAs whose completion wait timed out may still be writing tensor
+    // memory: no later tile issued any (ok stays false), so the commit of
+    // that tile is the last one; wait for its arrival before the
+    // deallocation (a second, longer bound).  MMAs finish in microseconds,
+    // so this only runs after a fault elsewhere; should even this wait give
+    // up, the memory is released all the same, because a CTA that exits
+    // holding tensor memory can block later allocations on its SM.
+    if (tid == 0 && mma_pending >= 0) {
+        uint32_t got = 0;
+        for (long it = 0; it < (1L << 30) && !got; it++) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(got)
+                : "r"(smem_u32(mbar)), "r"((uint32_t)mma_pending)
                 : "memory");
         }
     }

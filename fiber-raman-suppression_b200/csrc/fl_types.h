@@ -92,6 +92,7 @@ struct SlotState {
     int nsteps, ck_stride, seg, save_idx;
     int rec_pos;             // replayed steps within the current segment
     int stage;               // stage of the attempt in progress (0 = none)
+    int sub;                 // sub-segment (seg_cap steps) of the segment being replayed
     double cz, cdt;          // z and signed dt of the attempt in progress
     double aprop;            // adjoint: controller proposal before a segment clip
     double z, dt, qold;      // forward integrator
@@ -168,6 +169,7 @@ struct MmState {
     int phase, status;
     int cur, kperm, acur, akperm;
     int nsteps, ck_stride, seg, save_idx, rec_pos, stage;
+    int sub;                // sub-segment (seg_cap steps) of the segment being replayed
     double cz, cdt, aprop;
     double z, dt, qold;
     double az, adt, aqold;

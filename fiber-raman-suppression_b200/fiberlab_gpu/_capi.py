@@ -28,7 +28,8 @@ EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_forward_noalloc", "fl_mode_phase_gradient_batch",
            "fl_mode_phase_gradient_batch_device", "fl_server_create", "fl_server_destroy",
            "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_info_get",
-           "fl_problem_set_objective", "fl_forward_gain")
+           "fl_problem_set_objective", "fl_forward_gain", "fl_ctx_set_stream",
+           "fl_ctx_get_stream", "fl_forward_times")
 
 # device objectives (FL_OBJ_*) by the reference's objective names
 # (physics_models.jl:947-962); temporal_width runs with a host seed
@@ -109,6 +110,9 @@ def load() -> C.CDLL:
         lib.fl_ctx_launch_count.restype = C.c_long
         lib.fl_ctx_launch_count.argtypes = [vp]
         lib.fl_ctx_synchronize.argtypes = [vp]
+        lib.fl_ctx_set_stream.argtypes = [vp, vp]
+        lib.fl_ctx_get_stream.restype = vp
+        lib.fl_ctx_get_stream.argtypes = [vp]
         lib.fl_problem_create.argtypes = [vp, ip, ip, vp, vp, vp, vp, dp, dp, dp, dp, ip,
                                           C.POINTER(vp)]
         lib.fl_problem_destroy.argtypes = [vp]
@@ -122,6 +126,7 @@ def load() -> C.CDLL:
         lib.fl_mode_phase_gradient_batch.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_mode_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_rhs_eval.argtypes = [vp, ip, dp, vp, vp, vp]
+        lib.fl_forward_times.argtypes = [vp, vp, C.c_long, C.POINTER(C.c_long)]
         lib.fl_ctx_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.fl_server_create.argtypes = [vp, C.POINTER(FlServerOpts), C.POINTER(vp)]
         lib.fl_server_destroy.argtypes = [vp]
@@ -157,7 +162,7 @@ class Context:
     """fl_ctx on one device (one per host thread)."""
 
     def __init__(self, device: int = 0, checkpoints: int = 32, segment_steps: int = 16,
-                 step_log: int = 16384, max_iters: int = 100000, hbm_budget_bytes: int = 0):
+                 step_log: int = 0, max_iters: int = 100000, hbm_budget_bytes: int = 0):
         lib = load()
         self.opts = FlCtxOpts(hbm_budget_bytes, checkpoints, segment_steps, step_log, max_iters)
         h = C.c_void_p()
@@ -183,6 +188,21 @@ class Context:
 
     def synchronize(self):
         self.check(load().fl_ctx_synchronize(self.h))
+
+    def set_stream(self, stream=None):
+        """Run this context's calls on a caller stream (fl_ctx_set_stream):
+        a torch.cuda.Stream, a raw cudaStream_t handle (int), or None for the
+        context's private stream.  Handle 0 (torch's default stream) is the
+        legacy default stream and is passed as cudaStreamLegacy."""
+        h = getattr(stream, "cuda_stream", stream)
+        if stream is not None and h == 0:
+            h = 1  # cudaStreamLegacy
+        self.check(load().fl_ctx_set_stream(self.h, None if stream is None else int(h)))
+
+    @property
+    def stream(self) -> int:
+        """The raw handle of the stream the context's calls run on."""
+        return int(load().fl_ctx_get_stream(self.h) or 0)
 
     def close(self):
         if getattr(self, "h", None):
@@ -264,6 +284,14 @@ class GPUProblem:
         self.ctx.check(load().fl_forward(self.h, _ptr(u0), _ptr(z), len(z), _ptr(out),
                                          C.byref(st)))
         return out, st.as_dict()
+
+    def forward_times(self) -> np.ndarray:
+        """sol.t of the last forward: 0, every accepted step end, L."""
+        n = C.c_long()
+        self.ctx.check(load().fl_forward_times(self.h, None, 0, C.byref(n)))
+        t = np.empty(n.value)
+        self.ctx.check(load().fl_forward_times(self.h, _ptr(t), n.value, C.byref(n)))
+        return t
 
     def adjoint(self, lambdaL):
         lam = np.ascontiguousarray(lambdaL, dtype=np.complex128)

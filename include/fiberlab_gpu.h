@@ -60,8 +60,12 @@ typedef struct fl_server fl_server;
 typedef struct {
     size_t hbm_budget_bytes;   /* 0: no limit beyond cudaMalloc */
     int checkpoints;           /* z-checkpoint slots K for the adjoint (power of 2, default 32) */
-    int segment_steps;         /* forward steps kept per recompute segment (default 16) */
-    int step_log;              /* accepted-step log capacity (default 16384) */
+    int segment_steps;         /* dense-output steps kept per recompute sub-segment (default 16):
+                                  a solve of more than K x segment_steps accepted steps replays
+                                  each checkpoint segment once per sub-segment instead of
+                                  failing, so K and segment_steps trade memory for recompute */
+    int step_log;              /* accepted-step log capacity; 0 (default): max_iters entries,
+                                  so the log never ends a solve the step limit admits */
     long max_iters;            /* attempted steps per integration (default 100000, as maxiters) */
 } fl_ctx_opts;
 
@@ -92,6 +96,23 @@ long fl_ctx_launch_count(const fl_ctx *ctx);
 int fl_ctx_timing(const fl_ctx *ctx, double *last_call_ms, double *last_kernel_ms);
 /* Synchronise the context's stream. */
 int fl_ctx_synchronize(fl_ctx *ctx);
+/* Run every later call of this context on the caller's CUDA stream
+ * (a cudaStream_t passed as void*; NULL returns to the context's private
+ * stream; cudaStreamLegacy selects the legacy default stream).  Its work is
+ * then ordered with the caller's own work on that stream: a device-buffer
+ * entry point reads inputs that earlier work on the stream produced, without
+ * a host synchronisation in between.  The entry points still synchronise the
+ * stream before they return (they hand back statistics, and host-buffer
+ * calls their outputs).  Work already queued on the previous stream is
+ * waited for before the switch.  The reference's rule for concurrent solves
+ * is one solve with its own state per thread
+ * (agent-docs/current-agent-context/NUMERICS.md:35-37): here that is one
+ * context per host thread, each on its own stream;
+ * CUDA graphs the context captures are captured on its private stream and
+ * launched on the current one. */
+int fl_ctx_set_stream(fl_ctx *ctx, void *stream);
+/* The stream the context's calls currently run on. */
+void *fl_ctx_get_stream(const fl_ctx *ctx);
 
 /* Upload one resolved problem: the tables get_p_disp_mmf builds from the
  * `fiber`/`sim` dictionaries (simulate_disp_mmf.jl:87-114,
@@ -195,6 +216,14 @@ int fl_mode_phase_gradient_batch(fl_problem *prob, const double *u0, int nbatch,
                                  const double *phases, const unsigned char *mask, int log_cost,
                                  double *J, double *grad, fl_stats *stats);
 
+/* The accepted step positions of the last fl_forward of this problem: the
+ * reference's sol.t (the ODESolution's time points with dense output,
+ * simulate_disp_mmf.jl:190; used as sol.t by its callers), i.e. 0, the end
+ * of every accepted step, and L -- *n_out = naccept + 1 values, of which the
+ * first min(cap, *n_out) are written to t_out (cap 0 only queries the
+ * count).  FL_EINVAL without a completed preceding fl_forward. */
+int fl_forward_times(fl_problem *prob, double *t_out, long cap, long *n_out);
+
 /* One evaluation of the forward right-hand side disp_mmf!
  * (simulate_disp_mmf.jl:25-60) or, with adjoint = 1, of adjoint_disp_mmf!
  * (sensitivity_disp_mmf.jl:32-79) with the forward field u_fwd given
@@ -226,13 +255,16 @@ int fl_mode_phase_gradient_batch_device(fl_problem *prob, const double *d_u0, in
  *   receives Nt*nsave complex lab-frame spectra; stream 0 = default stream.
  * Everything else lives in one file-scope device array of 2 MiB that each GPU
  * loading the library holds until the process exits.  Limit: Nt <= 2^13
- * (larger grids return FL_EUNSUPPORTED) and 8192 accepted steps
- * (FL_ECAPACITY).  The first call on a device resolves the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call reuses the same array, so calls that overlap on the
- * GPU (other streams, other host threads) race; the state the solve needs
- * is re-initialised by each call.  Invalid save positions or a non-finite or
- * zero launch return FL_EINVAL. */
+ * (larger grids return FL_EUNSUPPORTED); being forward-only it keeps no step
+ * log, so the number of steps is bounded only by the attempted-step limit
+ * (100000, FL_MAXITERS).  The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture.  Every call reuses the same array, so calls that overlap
+ * on the GPU (other streams, other host threads) race; the state the solve
+ * needs is re-initialised by each call.  The calling thread's current device
+ * is restored before the call returns.  An error already pending on the
+ * thread is reported as FL_ECUDA and left pending.  Invalid save positions
+ * or a non-finite or zero launch return FL_EINVAL. */
 int fl_forward_noalloc(int device, int nt, const double *d_D, double gamma, const double *d_hR,
                        const double *d_selfsteep, double one_m_fR, double L, double reltol,
                        double abstol, const double *d_u0, const double *d_saveat, int nsave,
@@ -262,9 +294,10 @@ typedef struct {
     size_t hbm_budget_bytes;  /* slot workspaces (default 120 GB) */
     int evals_per_launch;     /* RHS evaluations per slot per launch (default 48) */
     int checkpoints;          /* per-slot z-checkpoints (power of 2, default 256) */
-    int segment_steps;        /* recompute segment length (default 128); a band-gradient
-                                 request holds up to checkpoints x segment_steps accepted
-                                 forward steps (FL_ECAPACITY beyond) */
+    int segment_steps;        /* recompute sub-segment length (default 128); a band-gradient
+                                 request of more than checkpoints x segment_steps accepted
+                                 forward steps recomputes more instead of failing; the step
+                                 log holds one entry per allowed attempted step (400000) */
     int max_active_ctas;      /* cap on requests in flight, counted in CTAs per transform (one
                                  per single-CTA slot, M x cluster CTAs per multimode slot);
                                  0: no cap beyond slots and the HBM budget */

@@ -17,7 +17,11 @@ from fiberlab_gpu import gain as G
 from fiberlab_gpu import problem as P
 from oracle import oracle as O
 
-REF_DATA = "/root/reference/src/gain_simulation"
+# A checkout of the reference project, when one is available: its Yb
+# cross-section data (src/gain_simulation/Yb_*.npz) then drives the
+# "reference" case; without it that case is skipped.
+REF_ROOT = os.environ.get("FIBERLAB_REFERENCE_ROOT", "")
+REF_DATA = os.path.join(REF_ROOT, "src", "gain_simulation") if REF_ROOT else ""
 
 
 def _synthetic_sections():
@@ -30,8 +34,9 @@ def _synthetic_sections():
 
 def _reference_sections():
     ab, em = (os.path.join(REF_DATA, f) for f in ("Yb_absorption.npz", "Yb_emission.npz"))
-    if not (os.path.exists(ab) and os.path.exists(em)):
-        pytest.skip("the reference's Yb cross-section data is not present")
+    if not (REF_DATA and os.path.exists(ab) and os.path.exists(em)):
+        pytest.skip("the reference's Yb cross-section data is not present "
+                    "(set FIBERLAB_REFERENCE_ROOT to a reference checkout)")
     a, e = np.load(ab), np.load(em)
     # get_ydfa_cross_sections: wavelength in nm, intensity x 1e-27 m²
     return (a["wavelength"] * 1e-9, a["intensity"] * 1e-27), (e["wavelength"] * 1e-9,

@@ -4,18 +4,28 @@ Hermite-Gauss problems (overlap tensor from the mode profiles, per-mode
 dispersion by mode group) at the oracle-sized shapes, the config-2 shape
 (M = 6, Nt = 2^12 over 5 ps, 1 m, 2 nJ) against the oracle, and the
 config-4 shape (M = 10, Nt = 2^14, 2 m, 5 nJ, 64 per-mode phase candidates)
-through size-independent properties: the same answer alone and in the
-batch, and the gradient against central differences of FP64 GPU forwards.
+through size-independent properties (the same answer alone and in the
+batch, the gradient against central differences of FP64 GPU forwards), and
+both configs' forward + adjoint gradients against golden fixtures of the
+FP64 oracle (tests/golden/make_multimode_fixtures.py).
 
 Tolerances: field relative L2 ≤ 1e-5 (FP32 mode) and ≤ 1e-10 (FP64 mode),
 Raman band fraction within 0.01 dB, gradient ≤ 1e-3 relative.
 """
+import os
+import sys
+
 import numpy as np
 import pytest
 
 from fiberlab_gpu import problem as P
 from fiberlab_gpu._capi import FiberLabGPUError, GPUProblem
 from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+if GOLDEN not in sys.path:
+    sys.path.insert(0, GOLDEN)
+import make_multimode_fixtures as MF  # noqa: E402  (the fixtures' problem definitions)
 
 pytestmark = pytest.mark.gpu
 
@@ -193,29 +203,98 @@ def test_mm_config4_shape_properties(gpu_ctx):
 
 def test_mm_config4_gradient_central_differences(gpu_ctx):
     # The adjoint gradient against central differences (h = 1e-4) on the
-    # config-4 shape, both in FP64 mode at tight tolerances (reltol 1e-10,
+    # config-4 shape along 4 random unit directions (no bias toward the
+    # gradient), both in FP64 mode at tight tolerances (reltol 1e-10,
     # abstol 1e-9): at the default tolerances the two sides differ by their
     # integration error (1e-4 .. 1e-3 on this 10-mode, 2 m problem), which
-    # is not what the check is after.  Directions mix a random unit vector
-    # with the gradient direction so that J(φ ± h d) differ well above the
-    # solves' noise.
+    # is not what the check is after.  The 8 FD costs run as one batch.
     fp = P.multimode_problem(3, 96, 16384, 10.0, 2.0, 5e-9, 200e-15, seed=0,
                              raman_threshold_thz=-2.0, reltol=1e-10, abstol=1e-9)
     rng = np.random.default_rng(44)
     ph = rng.standard_normal((10, fp.nt))
     gp64 = GPUProblem(gpu_ctx, fp, "fp64")
     J, g, _ = gp64.mode_phase_gradient_batch(ph[None])
+    d = rng.standard_normal((4, 10, fp.nt))
+    d /= np.linalg.norm(d.reshape(4, -1), axis=1)[:, None, None]
+    h = 1e-4
+    Jp, _, _ = gp64.mode_phase_gradient_batch(np.concatenate([ph + h * d, ph - h * d]))
+    fd = (Jp[:4] - Jp[4:]) / (2 * h)
+    ad = np.einsum("bmt,mt->b", d, g[0])
+    err = np.abs(fd - ad) / np.abs(fd)
+    assert np.all(err <= GRAD_TOL), (err, fd, ad)
 
-    def cost(p):
-        out, _ = gp64.forward(fp.uw0 * np.exp(1j * p))
-        return P.band_cost_and_seed(out[-1], fp.mask)[0]
-    for _ in range(2):
-        r = rng.standard_normal((10, fp.nt))
-        d = r / np.linalg.norm(r) + g[0] / np.linalg.norm(g[0])
-        d /= np.linalg.norm(d)
-        h = 1e-4
-        fd = (cost(ph + h * d) - cost(ph - h * d)) / (2 * h)
-        assert abs(fd - np.sum(g[0] * d)) <= GRAD_TOL * abs(fd)
+
+def test_mm_config2_against_oracle_fixture(gpu_ctx):
+    # config 2 (M = 6, Nt = 2^12 over 5 ps, 1 m, 2 nJ, Dirichlet(1) launch):
+    # FP32 forward + adjoint with per-mode phases N(0, 0.5²) against the FP64
+    # oracle's output field, band fraction and per-mode gradient
+    fx = np.load(os.path.join(GOLDEN, "mm_config2.npz"))
+    fp = MF.config2_problem()
+    ph = MF.config2_phases(fp)
+    gp = GPUProblem(gpu_ctx, fp)
+    out, st = gp.forward(fp.uw0 * np.exp(1j * ph))
+    assert rel(out[-1], fx["uL"]) < FIELD_TOL_FP32
+    J, g, gst = gp.mode_phase_gradient_batch(ph[None])
+    assert gst[0]["status"] == 0
+    assert abs(10 * np.log10(J[0]) - 10 * np.log10(float(fx["J"]))) < DB_TOL
+    assert rel(g[0], fx["grad"]) < GRAD_TOL, rel(g[0], fx["grad"])
+
+
+def test_mm_config4_against_oracle_fixture(gpu_ctx):
+    # config 4 (M = 10, Nt = 2^14 over 10 ps, 2 m, 5 nJ): 4 per-mode phase
+    # candidates N(0, 1) as one FP32 batch against the FP64 oracle's band
+    # fractions and gradients (on the bins where the launch is not
+    # negligible: the gradient vanishes with it), and candidate 0's field
+    fx = np.load(os.path.join(GOLDEN, "mm_config4.npz"))
+    fp = MF.config4_problem()
+    seeds = [int(x) for x in fx["seeds"]]
+    phs = np.stack([MF.config4_phases(fp, s) for s in seeds])
+    gp = GPUProblem(gpu_ctx, fp)
+    J, g, st = gp.mode_phase_gradient_batch(phs)
+    idx = fx["idx"]
+    for b in range(len(seeds)):
+        assert st[b]["status"] == 0
+        assert abs(10 * np.log10(J[b]) - 10 * np.log10(float(fx["J"][b]))) < DB_TOL
+        go = fx["grad"][b].astype(np.float64)
+        outside = np.ones(fp.nt, bool)
+        outside[idx] = False
+        e = np.sqrt(np.sum((g[b][:, idx] - go) ** 2) + np.sum(g[b][:, outside] ** 2))
+        assert e / np.linalg.norm(go) < GRAD_TOL, (b, e / np.linalg.norm(go))
+    out, _ = gp.forward(fp.uw0 * np.exp(1j * phs[0]))
+    assert rel(out[-1], fx["uL0"].astype(np.complex128)) < FIELD_TOL_FP32
+
+
+def test_mm_adjoint_beyond_checkpoint_capacity(gpu_ctx):
+    # the multimode stepper replays each checkpoint segment once per
+    # sub-segment when a solve has more accepted steps than checkpoints x
+    # segment_steps
+    from fiberlab_gpu._capi import Context
+    fp = hg_problem(3, 256, L=0.5, energy=6e-9)
+    phi = 0.5 * np.random.default_rng(32).standard_normal(fp.nt)
+    J, g, st = GPUProblem(Context(0, checkpoints=2, segment_steps=3), fp).phase_gradient_batch(
+        phi[None, :])
+    assert st[0]["status"] == 0 and st[0]["naccept"] > 6
+    Jo, go, _ = O.phase_gradient(fp, phi)
+    assert abs(10 * np.log10(J[0]) - 10 * np.log10(Jo)) < DB_TOL
+    assert rel(g[0], go) < GRAD_TOL
+
+
+def test_mm_save_on_interior_step_end(gpu_ctx):
+    # the multimode stepper's dense output at a save position exactly on an
+    # interior accepted step end (sol.t from a first forward)
+    fp = hg_problem(3, 256, L=0.5, energy=6e-9)
+    gp = GPUProblem(gpu_ctx, fp)
+    gp.forward()
+    t = gp.forward_times()
+    assert t[0] == 0.0 and t[-1] == fp.L and np.all(np.diff(t) > 0)
+    zk = float(t[len(t) // 2])
+    zs = [0.0, np.nextafter(zk, 0.0), zk, np.nextafter(zk, 1.0), fp.L]
+    out, st = gp.forward(saveat=zs)
+    np.testing.assert_array_equal(gp.forward_times(), t)
+    ref, _, _ = O.forward(fp, zsave=zs)
+    for i in range(len(zs)):
+        assert rel(out[i], ref[i]) < FIELD_TOL_FP32, (i, rel(out[i], ref[i]))
+    assert rel(out[1], out[2]) < 1e-6 and rel(out[3], out[2]) < 1e-6
 
 
 def test_mm_grin_fiber_forward(gpu_ctx):

@@ -148,6 +148,29 @@ def test_saveat_dense_output(gpu_ctx):
         assert rel(out[i], ref[i]) < FIELD_TOL_FP32
 
 
+def test_save_on_interior_step_end(gpu_ctx):
+    # a save position exactly on the end of an accepted interior step is taken
+    # from that step's dense output (not skipped): sol.t of a first forward
+    # gives the step ends, the second forward with a save on one of them
+    # takes the same steps and matches the oracle's dense output there and
+    # the saves one ulp to either side
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6)
+    gp = GPUProblem(gpu_ctx, fp)
+    gp.forward()
+    t = gp.forward_times()
+    assert t[0] == 0.0 and t[-1] == fp.L and np.all(np.diff(t) > 0)
+    zk = float(t[len(t) // 2])
+    zs = [0.0, np.nextafter(zk, 0.0), zk, np.nextafter(zk, 1.0), fp.L]
+    out, st = gp.forward(saveat=zs)
+    assert st["status"] == 0
+    np.testing.assert_array_equal(gp.forward_times(), t)
+    ref, _, _ = O.forward(fp, zsave=zs)
+    for i in range(len(zs)):
+        assert rel(out[i], ref[i]) < FIELD_TOL_FP32, (i, rel(out[i], ref[i]))
+    assert rel(out[1], out[2]) < 1e-6 and rel(out[3], out[2]) < 1e-6
+
+
 def test_seeded_adjoint_matches_oracle(gpu_ctx):
     fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
                                rep_rate_hz=80.5e6)
@@ -218,6 +241,28 @@ def test_gradient_central_differences(gpu_ctx):
         assert abs(fd - g[0] @ d) <= GRAD_TOL * abs(fd) + 1e-12
 
 
+def test_gradient_central_differences_config1(gpu_ctx):
+    # config 1 itself (Nt = 2^13 over 10 ps, 0.5 m, 0.1 W at 80 MHz, band
+    # < -13 THz, phase N(0, 0.5²) seed 0): the FP32 product gradient against
+    # central differences (h = 1e-4) along 8 random unit directions, with no
+    # bias toward the gradient.  The 16 FD costs come from one batched
+    # FP64-mode launch.
+    fp = cfg0()
+    rng = np.random.default_rng(0)
+    phi = 0.5 * rng.standard_normal(fp.nt)
+    J, g, _ = GPUProblem(gpu_ctx, fp).phase_gradient_batch(phi[None, :])
+    drng = np.random.default_rng(8)
+    d = drng.standard_normal((8, fp.nt))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    h = 1e-4
+    probes = np.concatenate([phi + h * d, phi - h * d])
+    Jp, _, _ = GPUProblem(gpu_ctx, fp, "fp64").phase_gradient_batch(probes)
+    fd = (Jp[:8] - Jp[8:]) / (2 * h)
+    ad = d @ g[0]
+    err = np.abs(fd - ad) / np.abs(fd)
+    assert np.all(err <= GRAD_TOL), (err, fd, ad)
+
+
 def test_batch_results_equal_alone_and_in_mix(gpu_ctx):
     fp = P.single_mode_problem(nt=2048, time_window_ps=10.0, L=0.5, power_w=0.1,
                                rep_rate_hz=80.5e6)
@@ -234,7 +279,7 @@ def test_batch_results_equal_alone_and_in_mix(gpu_ctx):
 def test_status_codes_without_a_fault(gpu_ctx):
     # host-side injections, no GPU fault: non-Hermitian hR is rejected at
     # upload; a huge γ overflows the field -> FL_NONFINITE; a tiny iteration
-    # cap -> FL_MAXITERS; a tiny segment cap -> FL_ECAPACITY
+    # cap -> FL_MAXITERS; a step log smaller than the solve -> FL_ECAPACITY
     fp = P.single_mode_problem(nt=256, time_window_ps=3.0, L=0.3, power_w=0.1,
                                rep_rate_hz=80.5e6)
     bad = P.FiberProblem(**{**fp.__dict__})
@@ -254,8 +299,7 @@ def test_status_codes_without_a_fault(gpu_ctx):
     long = P.single_mode_problem(nt=256, time_window_ps=3.0, L=3.0, power_w=0.3,
                                  rep_rate_hz=80.5e6)
     with pytest.raises(FiberLabGPUError) as e:
-        GPUProblem(Context(0, checkpoints=2, segment_steps=1), long).phase_gradient_batch(
-            np.zeros((1, long.nt)))
+        GPUProblem(Context(0, step_log=4), long).phase_gradient_batch(np.zeros((1, long.nt)))
     assert e.value.status == 9
     # objective codes and the worst-mode smoothness are checked at the boundary
     from fiberlab_gpu._capi import load
@@ -264,6 +308,24 @@ def test_status_codes_without_a_fault(gpu_ctx):
         with pytest.raises(FiberLabGPUError) as e:
             gp.ctx.check(load().fl_problem_set_objective(gp.h, code, tau))
         assert e.value.status == 1
+
+
+@pytest.mark.parametrize("caps", [(2, 1), (4, 3), (8, 5)])
+def test_adjoint_beyond_checkpoint_capacity(gpu_ctx, caps):
+    # more accepted steps than checkpoints x segment_steps: each checkpoint
+    # segment is replayed once per sub-segment of segment_steps steps (no
+    # FL_ECAPACITY); the gradient matches the oracle and the default layout
+    K, seg = caps
+    fp = P.single_mode_problem(nt=256, time_window_ps=3.0, L=3.0, power_w=0.3,
+                               rep_rate_hz=80.5e6, raman_threshold_thz=-3.0)
+    phi = 0.3 * np.random.default_rng(31).standard_normal(fp.nt)
+    J, g, st = GPUProblem(Context(0, checkpoints=K, segment_steps=seg), fp).phase_gradient_batch(
+        phi[None, :])
+    assert st[0]["status"] == 0 and st[0]["naccept"] > K * seg
+    Jd, gd, _ = GPUProblem(gpu_ctx, fp).phase_gradient_batch(phi[None, :])
+    Jo, go, _ = O.phase_gradient(fp, phi)
+    assert J[0] == Jd[0]                      # the forward is the same solve
+    assert rel(g[0], go) < GRAD_TOL and rel(g[0], gd[0]) < GRAD_TOL
 
 
 def test_physical_gradient_phase_amplitude_energy(gpu_ctx):

@@ -3,14 +3,15 @@
 fl_forward_noalloc is for callers that cannot call cudaMalloc (a host runtime
 whose device memory belongs to its own pool allocator, or a request loop that
 must not take cudaMalloc's device synchronisation): it runs on device buffers
-the caller owns and keeps its own state in a fixed 2 MiB device array.  This
+the caller owns and keeps its own state in a fixed 2 MiB device array (its
+only limit is Nt <= 2^13: being forward-only it keeps no step log).  This
 file is collected last so that a failure here comes after every other test.
 """
 import numpy as np
 import pytest
 
 from fiberlab_gpu import problem as P
-from fiberlab_gpu._capi import GPUProblem, forward_noalloc
+from fiberlab_gpu._capi import Context, GPUProblem, forward_noalloc
 
 pytestmark = pytest.mark.gpu
 
@@ -55,6 +56,26 @@ def test_forward_noalloc_matches_forward(gpu_ctx):
             err = np.linalg.norm(out[i] - ref[i]) / np.linalg.norm(ref[i])
             assert err < FIELD_TOL_FP32, (fp.nt, zs[i], err)
         assert st["z_end"] == fp.L and st["naccept"] > 0
+
+
+def test_forward_noalloc_long_solve_has_no_step_limit():
+    # a forward-only solve keeps no step log: 1 W (5.9 kW peak) over 3 m of
+    # SMF-28 on 2^11 points takes about 10^4 accepted steps, more than a
+    # fixed step log of 8192 entries would hold, and still matches fl_forward
+    # (run here with a step log large enough for its adjoint checkpoints)
+    torch = pytest.importorskip("torch")
+    fp = P.single_mode_problem(nt=2048, time_window_ps=10.0, L=3.0, power_w=1.0, rep_rate_hz=80e6,
+                               validate_grid=False)
+    zs = [0.0, 1.5, 3.0]
+    ref, rst = GPUProblem(Context(0, step_log=1 << 16), fp).forward(saveat=zs)
+    b = _device_inputs(torch, fp, zs)
+    rc, st = _run(b, fp, zs)
+    assert rc == 0, rc
+    assert st["naccept"] > 8192 and rst["naccept"] > 8192, (st, rst)
+    out = b["out"].cpu().numpy().view(np.complex128).reshape(len(zs), 1, fp.nt)
+    for i in range(len(zs)):
+        err = np.linalg.norm(out[i] - ref[i]) / np.linalg.norm(ref[i])
+        assert err < FIELD_TOL_FP32, (zs[i], err)
 
 
 def test_forward_noalloc_rejects_oversize_and_bad_input(gpu_ctx):
