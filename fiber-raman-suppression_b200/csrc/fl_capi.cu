@@ -20,6 +20,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/fiberlab_gpu.h"
 #include "fl_launch.h"
 #include "fl_mm_launch.h"
@@ -39,6 +41,17 @@ struct fl_ctx {
 };
 
 namespace {
+
+// NVTX range over a scope: the phases of a call (stepper launches,
+// evaluation rounds, server launches, evidence) show up as named ranges in
+// Nsight Systems and as ncu's --nvtx filter; without a tool attached a
+// push/pop is a no-op call.
+struct Nvtx {
+    explicit Nvtx(const char* name) { nvtxRangePushA(name); }
+    ~Nvtx() { nvtxRangePop(); }
+    Nvtx(const Nvtx&) = delete;
+    Nvtx& operator=(const Nvtx&) = delete;
+};
 
 int set_err(fl_ctx* c, int code, const char* fmt, ...) {
     if (c) {
@@ -151,6 +164,9 @@ struct fl_problem {
     // device staging of the host-buffer batch calls (grow-only, reused)
     char* d_stage = nullptr;
     size_t stage_bytes = 0;
+    // evidence reductions of the last forward's save positions (grow-only)
+    double* d_ev = nullptr;
+    size_t ev_bytes = 0;
     // workspace of the last forward (kept for fl_adjoint)
     struct Work* last = nullptr;
     struct MmWork* mlast = nullptr;        // same for multimode problems
@@ -324,6 +340,7 @@ int launch_slots(fl_ctx* ctx, fl_problem* pr, Work* w, int nactive, int max_eval
 }
 
 int run_to_completion(fl_problem* pr, Work* w) {
+    Nvtx nvtx_("fl: single-mode stepper (run to completion)");
     fl_ctx* ctx = pr->ctx;
     CU(cudaEventRecord(ctx->ev[2], ctx->stream));
     int rc = launch_slots(ctx, pr, w, w->B, 0x7fffffff);
@@ -355,6 +372,7 @@ void fill_stats(const SlotState& s, fl_stats* o) {
     o->checkpoints_used = s.ck_stride > 0 ? (s.nsteps + s.ck_stride - 1) / s.ck_stride : 0;
     o->J = s.J;
     o->z_end = s.z;
+    o->recompute_steps = s.nrec;
 }
 
 int check_problem(fl_problem* pr) {
@@ -630,6 +648,7 @@ MmRound mm_round_args(fl_problem* pr, MmWork* w, int nactive) {
 // has its own attempted-step limits, so the loop ends; the host bound below
 // only guards against a control bug.
 int mm_run(fl_problem* pr, MmWork* w, int nactive) {
+    Nvtx nvtx_("fl: multimode evaluation rounds");
     fl_ctx* ctx = pr->ctx;
     MmRoundFn round = mm_round_launcher(ilog2i(pr->nt));
     if (!round) return set_err(ctx, FL_EUNSUPPORTED, "multimode Nt = %d is not built", pr->nt);
@@ -726,6 +745,7 @@ void mm_fill_stats(const MmState& s, fl_stats* o) {
     o->checkpoints_used = s.ck_stride > 0 ? (s.nsteps + s.ck_stride - 1) / s.ck_stride : 0;
     o->J = s.J;
     o->z_end = s.z;
+    o->recompute_steps = s.nrec;
 }
 
 __global__ void mm_gather_J_kernel(const MmState* __restrict__ st, int n, double* __restrict__ J) {
@@ -793,12 +813,22 @@ int mm_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave
                double* out_spectra, fl_stats* stats) {
     fl_ctx* ctx = pr->ctx;
     const size_t nm = (size_t)pr->nt * pr->m;
-    delete pr->mlast;
-    pr->mlast = nullptr;
-    MmWork* w = nullptr;
-    int rc = mm_work_create(pr, 1, nsave, MODE_FORWARD, 0, &w);
-    if (rc) return rc;
-    pr->mlast = w;
+    // the problem's one-slot forward workspace is reused by later forwards
+    // with the same number of save positions (no allocation per call)
+    MmWork* w = pr->mlast;
+    int rc = FL_OK;
+    if (w && w->B == 1 && w->nsave == nsave && !w->per_mode) {
+        rc = mm_set_mode(ctx, w, MODE_FORWARD, 0);
+        if (rc) return rc;
+        CU(cudaMemsetAsync(w->d_state, 0, sizeof(MmState), ctx->stream));
+    } else {
+        delete pr->mlast;
+        pr->mlast = nullptr;
+        w = nullptr;
+        rc = mm_work_create(pr, 1, nsave, MODE_FORWARD, 0, &w);
+        if (rc) return rc;
+        pr->mlast = w;
+    }
     CU(cudaMemcpyAsync(w->d_u0, u0, 16 * nm, cudaMemcpyHostToDevice, ctx->stream));
     if (nsave)
         CU(cudaMemcpyAsync(w->d_zsave, saveat, 8 * (size_t)nsave, cudaMemcpyHostToDevice,
@@ -871,6 +901,7 @@ int mm_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const
 int mm_phase_gradient_device(fl_problem* pr, const double* d_u0, int nbatch,
                              const double* d_phases, int per_mode, const unsigned char* d_mask,
                              int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+    Nvtx nvtx_("fl: multimode batched forward + adjoint + gradient");
     fl_ctx* ctx = pr->ctx;
     const int nt = pr->nt;
     const size_t nm = (size_t)nt * pr->m;
@@ -1088,6 +1119,7 @@ int srv_new_chunk(fl_server* sv, SrvBucket* b) {
 
 // place request r into free slot i of chunk c (stream-ordered before the next launch)
 int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
+    Nvtx nvtx_("fl: server admit");
     fl_ctx* ctx = sv->ctx;
     const fl_problem* pr = r->prob;
     const size_t nm = (size_t)b->nt * b->m;
@@ -1155,6 +1187,7 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
 // (the status is published under the server lock by the caller)
 int srv_retire(fl_server* sv, SrvBucket* b, SrvChunk* c,
                std::vector<std::pair<SrvRequest*, int>>& done) {
+    Nvtx nvtx_("fl: server retire");
     fl_ctx* ctx = sv->ctx;
     const size_t nm = (size_t)b->nt * b->m;
     if (c->mm) {
@@ -1201,6 +1234,7 @@ int srv_retire(fl_server* sv, SrvBucket* b, SrvChunk* c,
 }
 
 int srv_launch(fl_server* sv, SrvBucket* b, SrvChunk* c) {
+    Nvtx nvtx_("fl: server launch");
     fl_ctx* ctx = sv->ctx;
     const int logn = ilog2i(b->nt);
     if (c->mm) {
@@ -1414,7 +1448,7 @@ int fl_ctx_create(int device, const fl_ctx_opts* opts, fl_ctx** out) {
     ctx->device = device;
     ctx->opts.hbm_budget_bytes = 0;
     ctx->opts.checkpoints = 32;
-    ctx->opts.segment_steps = 16;
+    ctx->opts.segment_steps = 64;
     ctx->opts.step_log = 0;  // one entry per allowed attempted step
     ctx->opts.max_iters = 100000;
     if (opts) {
@@ -1564,6 +1598,7 @@ int fl_problem_destroy(fl_problem* pr) {
     delete pr->last;
     delete pr->mlast;
     cudaFree(pr->d_stage);
+    cudaFree(pr->d_ev);
     cudaFree(pr->d_G[0]);
     cudaFree(pr->d_G[1]);
     cudaFree(pr->d_Ga);
@@ -1581,6 +1616,7 @@ int fl_problem_destroy(fl_problem* pr) {
 int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, const double* u0,
                     const double* saveat, int nsave, double* out_spectra, double* out_pump,
                     fl_stats* stats) {
+    Nvtx nvtx_("fl_forward_gain");
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
@@ -1739,6 +1775,7 @@ int fl_forward_gain(fl_problem* pr, const fl_gain* gain, double pump_power, cons
 
 int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave,
                double* out_spectra, fl_stats* stats) {
+    Nvtx nvtx_("fl_forward");
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
@@ -1764,12 +1801,21 @@ int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave
     if (!(nrm > 0)) return set_err(ctx, FL_EINVAL, "input spectrum must be nonzero");
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
     if (pr->use_mm) return mm_forward(pr, u0, saveat, nsave, out_spectra, stats);
-    delete pr->last;
-    pr->last = nullptr;
-    Work* w = nullptr;
-    rc = new_work(pr, 1, nsave, MODE_FORWARD, &w);
-    if (rc) return rc;
-    pr->last = w;
+    // the problem's one-slot forward workspace is reused by later forwards
+    // with the same number of save positions (no allocation per call)
+    Work* w = pr->last;
+    if (w && w->B == 1 && w->nsave == nsave) {
+        rc = set_mode(ctx, w, MODE_FORWARD, 0);
+        if (rc) return rc;
+        CU(cudaMemsetAsync(w->d_state, 0, sizeof(SlotState), ctx->stream));
+    } else {
+        delete pr->last;
+        pr->last = nullptr;
+        w = nullptr;
+        rc = new_work(pr, 1, nsave, MODE_FORWARD, &w);
+        if (rc) return rc;
+        pr->last = w;
+    }
     CU(cudaMemcpyAsync(w->d_u0, u0, 16 * (size_t)nt, cudaMemcpyHostToDevice, ctx->stream));
     if (nsave)
         CU(cudaMemcpyAsync(w->d_zsave, saveat, 8 * (size_t)nsave, cudaMemcpyHostToDevice,
@@ -1787,6 +1833,7 @@ int fl_forward(fl_problem* pr, const double* u0, const double* saveat, int nsave
 }
 
 int fl_adjoint(fl_problem* pr, const double* lambdaL, double* lambda0, fl_stats* stats) {
+    Nvtx nvtx_("fl_adjoint");
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
@@ -1866,8 +1913,62 @@ int fl_forward_times(fl_problem* pr, double* t_out, long cap, long* n_out) {
     return FL_OK;
 }
 
+int fl_forward_evidence(fl_problem* pr, int nsave, double* ev_out) {
+    Nvtx nvtx_("fl_forward_evidence");
+    int rc = check_problem(pr);
+    if (rc) return rc;
+    fl_ctx* ctx = pr->ctx;
+    if (!ev_out || nsave < 1) return set_err(ctx, FL_EINVAL, "null argument");
+    const int M = pr->m, nt = pr->nt;
+    const double* d_save = nullptr;
+    int status = FL_EINVAL;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
+    if (pr->use_mm) {
+        MmWork* w = pr->mlast;
+        if (w && w->B == 1 && w->nsave == nsave) {
+            std::vector<MmState> st;
+            rc = mm_read_states(ctx, w, 1, st);
+            if (rc) return rc;
+            status = st[0].phase == PH_DONE ? st[0].status : FL_EINVAL;
+            d_save = w->d_save;
+        }
+    } else {
+        Work* w = pr->last;
+        if (w && w->B == 1 && w->nsave == nsave) {
+            std::vector<SlotState> st;
+            rc = read_states(ctx, w, st);
+            if (rc) return rc;
+            status = st[0].phase == PH_DONE ? st[0].status : FL_EINVAL;
+            d_save = w->d_save;
+        }
+    }
+    if (!d_save || status != FL_OK)
+        return set_err(ctx, FL_EINVAL,
+                       "fl_forward_evidence needs a completed fl_forward with %d save positions",
+                       nsave);
+    EvidenceFn fn = mm_evidence_launcher(ilog2i(nt));
+    if (!fn) return set_err(ctx, FL_EUNSUPPORTED, "evidence for Nt = %d is not built", nt);
+    const size_t bytes = sizeof(double) * (size_t)nsave * (kEvFixed + M);
+    if (bytes > pr->ev_bytes) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        cudaFree(pr->d_ev);
+        pr->d_ev = nullptr;
+        pr->ev_bytes = 0;
+        CU(cudaMalloc(&pr->d_ev, bytes));
+        pr->ev_bytes = bytes;
+    }
+    EvidenceArgs a{pr->d_tw[1], static_cast<const double*>(pr->d_ss[1]), d_save, nsave, M, nt,
+                   pr->d_ev, ctx->stream};
+    CU(fn(a));
+    ctx->launches++;
+    CU(cudaMemcpyAsync(ev_out, pr->d_ev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
+    return FL_OK;
+}
+
 int fl_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const double* u_fwd,
                 double* du_out) {
+    Nvtx nvtx_("fl_rhs_eval");
     int rc = check_problem(pr);
     if (rc) return rc;
     fl_ctx* ctx = pr->ctx;
@@ -1901,6 +2002,7 @@ int fl_rhs_eval(fl_problem* pr, int adjoint, double z, const double* u_in, const
 static int phase_gradient_core(fl_problem* pr, Work* w, int nbatch, const double* d_u0,
                                const double* d_phases, const unsigned char* d_mask,
                                int log_cost, double* d_J, double* d_grad, fl_stats* stats) {
+    Nvtx nvtx_("fl: batched forward + adjoint + gradient");
     fl_ctx* ctx = pr->ctx;
     const int nt = pr->nt;
     CU(cudaEventRecord(ctx->ev[0], ctx->stream));

@@ -792,6 +792,7 @@ struct MmCtl {
                 st.cur ^= 1;
                 st.kperm ^= 1;
                 st.rec_pos++;
+                st.nrec++;
                 const SubSeg sb = sub_segment(d, st);
                 if (sb.seg_lo + st.rec_pos >= sb.hi) st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
                 return;
@@ -1162,6 +1163,8 @@ struct MmCtl {
             return;
         }
         st.abstol_adj = scl == 0.0 ? d.abstol : d.abstol * scl;  // sensitivity_disp_mmf.jl:324-325
+        st.nrec = 0;
+        st.dense = 0;
         st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
         st.sub = last_sub(d, st, st.seg);
         st.acur = 0;

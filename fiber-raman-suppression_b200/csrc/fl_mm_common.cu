@@ -22,6 +22,20 @@ MmRoundFn mm_round_launcher(int logn) {
     return f[logn];
 }
 
+#define DECL_EV(LOGN) cudaError_t mm_evidence_##LOGN(const EvidenceArgs&);
+DECL_EV(6) DECL_EV(7) DECL_EV(8) DECL_EV(9) DECL_EV(10) DECL_EV(11) DECL_EV(12) DECL_EV(13)
+DECL_EV(14) DECL_EV(15)
+#undef DECL_EV
+
+EvidenceFn mm_evidence_launcher(int logn) {
+    static const EvidenceFn f[16] = {nullptr,        nullptr,        nullptr,        nullptr,
+                                     nullptr,        nullptr,        mm_evidence_6,  mm_evidence_7,
+                                     mm_evidence_8,  mm_evidence_9,  mm_evidence_10, mm_evidence_11,
+                                     mm_evidence_12, mm_evidence_13, mm_evidence_14, mm_evidence_15};
+    if (logn < 0 || logn > 15) return nullptr;
+    return f[logn];
+}
+
 int mm_cluster_ctas(int logn) { return logn == 15 ? 4 : 1; }
 
 bool mm_supported_modes(int M) { return M >= 2 && M <= 10; }

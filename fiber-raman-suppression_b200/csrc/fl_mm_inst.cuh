@@ -1,5 +1,8 @@
 // fl_mm_inst.cuh -- instantiation helper of the multimode evaluation round.
 #pragma once
+#include <nvtx3/nvToolsExt.h>
+
+#include "fl_evidence.cuh"
 #include "fl_mm.cuh"
 #include "fl_mm_launch.h"
 
@@ -39,21 +42,40 @@ cudaError_t mm_launch_fft_kernels(const MmRound& a, int which) {
     }
 }
 
+// one evaluation round; each stage's launches sit in a named NVTX range
+// (host-side: under graph capture the ranges mark the capture)
 template <int LOGN, int LOGE, int CL>
 cudaError_t mm_round(const MmRound& a) {
     cudaError_t e;
 #define FL_TRY(x)                        \
-    if ((e = (x)) != cudaSuccess) return e;
+    if ((e = (x)) != cudaSuccess) {      \
+        nvtxRangePop();                  \
+        return e;                        \
+    }
+    nvtxRangePushA("fl: mm prologue");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 0)));
     FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 0)));
+    nvtxRangePop();
+    nvtxRangePushA("fl: mm Im X contraction");
     FL_TRY(mm_launch_contract(a, 1));
+    nvtxRangePop();
+    nvtxRangePushA("fl: mm pairs");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 1)));
     FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 1)));
+    nvtxRangePop();
+    nvtxRangePushA("fl: mm contraction");
     FL_TRY(mm_launch_contract(a, 0));
     FL_TRY(mm_launch_contract(a, 2));
+    nvtxRangePop();
+    nvtxRangePushA("fl: mm epilogue");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 2)));
     FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 2)));
-    if (a.control) FL_TRY(mm_launch_control(a, 1));
+    nvtxRangePop();
+    if (a.control) {
+        nvtxRangePushA("fl: mm control");
+        FL_TRY(mm_launch_control(a, 1));
+        nvtxRangePop();
+    }
 #undef FL_TRY
     return cudaSuccess;
 }
@@ -63,4 +85,7 @@ cudaError_t mm_round(const MmRound& a) {
 #define FL_MM_INSTANCE(LOGN, LOGE, CL)                                                     \
     namespace fl {                                                                         \
     cudaError_t mm_round_##LOGN(const MmRound& a) { return mm_round<LOGN, LOGE, CL>(a); } \
+    cudaError_t mm_evidence_##LOGN(const EvidenceArgs& a) {                                \
+        return launch_evidence<LOGN, LOGE, CL>(a);                                         \
+    }                                                                                      \
     }

@@ -23,6 +23,23 @@ struct MmRound {
 
 using MmRoundFn = cudaError_t (*)(const MmRound&);
 
+// Evidence reductions over saved spectra (fl_evidence.cuh).  Values per save
+// position: [Σ tpow, max tpow, temporal edge sum, Σ spow, spectral edge sum,
+// Σ |u|²/|ss|, then the M per-mode Σ_t |fft(u_m)|²], tpow and spow the
+// mode-summed temporal and spectral power.
+constexpr int kEvFixed = 6;
+struct EvidenceArgs {
+    const void* tw;          // FP64 twiddles exp(-2 pi i k / Nt)
+    const double* ss;        // FP64 fftshift(ωs/ω0) (|ωs| = |ss| ω0)
+    const double* spectra;   // nsave x M x Nt complex doubles, lab frame
+    int nsave, M, N;
+    double* out;             // nsave x (kEvFixed + M), device
+    cudaStream_t stream;
+};
+using EvidenceFn = cudaError_t (*)(const EvidenceArgs&);
+// evidence launcher for Nt = 2^logn (nullptr when not built)
+EvidenceFn mm_evidence_launcher(int logn);
+
 // evaluation round for Nt = 2^logn (nullptr when not built)
 MmRoundFn mm_round_launcher(int logn);
 // the grid-size-independent kernels (common translation unit)

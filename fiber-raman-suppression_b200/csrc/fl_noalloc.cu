@@ -198,6 +198,7 @@ extern "C" int fl_forward_noalloc(int device, int nt, const double* d_D, double 
         stats->checkpoints_used = 0;
         stats->J = 0.0;
         stats->z_end = st.z;
+        stats->recompute_steps = 0;
     }
     return st.status;
 }

@@ -570,6 +570,11 @@ struct SubSeg {
 template <class Desc, class State>
 __device__ __forceinline__ SubSeg sub_segment(const Desc& d, const State& st) {
     SubSeg r;
+    if (st.dense) {  // the forward kept the interpolant of every step: one range
+        r.seg_lo = r.lo = 0;
+        r.seg_hi = r.hi = st.nsteps;
+        return r;
+    }
     r.seg_lo = st.seg * st.ck_stride;
     r.seg_hi = min(r.seg_lo + st.ck_stride, st.nsteps);
     r.lo = r.seg_lo + st.sub * d.seg_cap;
@@ -581,6 +586,49 @@ template <class Desc, class State>
 __device__ __forceinline__ int last_sub(const Desc& d, const State& st, int seg) {
     const int lo = seg * st.ck_stride, hi = min(lo + st.ck_stride, st.nsteps);
     return (hi - lo - 1) / d.seg_cap;
+}
+
+// Dense interpolant of an accepted step into sg (5 fields): c0 = ũ_n,
+// c_p = Σ_i r_ip k_i (Tsit5's free 4th-order interpolant), read stage-outer
+// over chunks of 4 points per thread as in stage_input.
+template <typename RF, int LOGN, int LOGE>
+__device__ __forceinline__ void store_interp(const SlotDesc& d, const double* u, int kperm,
+                                             cx<RF>* sg) {
+    using S = FftShape<LOGN, LOGE>;
+    using Sol = SmSolver<RF, LOGN, LOGE>;
+    using CF = cx<RF>;
+    constexpr int N = S::N, E = S::E;
+    constexpr int RC = E < 4 ? E : 4;
+    static_assert(E % RC == 0, "chunks tile the thread's points");
+#pragma unroll
+    for (int s0 = 0; s0 < E; s0 += RC) {
+        double cr[RC][4], ci[RC][4];
+#pragma unroll
+        for (int c = 0; c < RC; c++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) cr[c][q] = ci[c][q] = 0.0;
+#pragma unroll 1
+        for (int i = 0; i < 7; i++) {
+            const CF* __restrict__ kv = Sol::kp(d.kf, kperm, i);
+            CF x[RC];
+#pragma unroll
+            for (int c = 0; c < RC; c++) x[c] = kv[Sol::bin(s0 + c)];
+#pragma unroll
+            for (int c = 0; c < RC; c++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    cr[c][q] += kT5r[i][q] * (double)x[c].re;
+                    ci[c][q] += kT5r[i][q] * (double)x[c].im;
+                }
+        }
+#pragma unroll
+        for (int c = 0; c < RC; c++) {
+            const int b = Sol::bin(s0 + c);
+            sg[b] = down<RF>(ld2(u, b));
+#pragma unroll
+            for (int q = 0; q < 4; q++) sg[(q + 1) * N + b] = mk((RF)cr[c][q], (RF)ci[c][q]);
+        }
+    }
 }
 
 template <typename RF, int LOGN, int LOGE>
@@ -766,11 +814,22 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 continue;
             }
             st.abstol_adj = scl == 0.0 ? d.abstol : d.abstol * scl;  // sensitivity_disp_mmf.jl:324-325
-            st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
-            st.sub = last_sub(d, st, st.seg);
             st.acur = 0;
             st.akperm = 0;
             st.a_naccept = st.a_nreject = st.a_nf = st.a_iters = 0;
+            st.nrec = 0;
+            // every step's interpolant is in the buffer when the forward fit it
+            // (kept by the forward; an earlier adjoint of this solve then did
+            // not overwrite it)
+            st.dense = st.nsteps <= d.seg_cap ? 1 : 0;
+            if (st.dense) {
+                st.seg = 0;
+                st.sub = 0;
+                st.phase = PH_ADJ_INIT;
+                continue;
+            }
+            st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
+            st.sub = last_sub(d, st, st.seg);
             restore_checkpoint<RF, LOGN, LOGE>(d, st.seg, st);
             st.phase = PH_REC;
             continue;
@@ -983,48 +1042,17 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
             const double z = st.cz, dt = st.cdt;
             const double* u = d.u[st.cur];
             if (rec) {
-                // interpolant of this step: c0 = ũ_n, c_p = Σ_i r_ip k_i
-                // (stage-outer over chunks of 4 points, as in stage_input),
-                // kept only for the steps of the current sub-segment
+                // interpolant of this step, kept only for the steps of the
+                // current sub-segment
                 const SubSeg sb = sub_segment(d, st);
                 const int n = sb.seg_lo + st.rec_pos;
-                CF* sg = (CF*)d.seg + (size_t)max(n - sb.lo, 0) * 5 * N;
-                constexpr int RC = E < 4 ? E : 4;
-                static_assert(E % RC == 0, "chunks tile the thread's points");
                 if (n >= sb.lo)
-#pragma unroll
-                for (int s0 = 0; s0 < E; s0 += RC) {
-                    double cr[RC][4], ci[RC][4];
-#pragma unroll
-                    for (int c = 0; c < RC; c++)
-#pragma unroll
-                        for (int q = 0; q < 4; q++) cr[c][q] = ci[c][q] = 0.0;
-#pragma unroll 1
-                    for (int i = 0; i < 7; i++) {
-                        const CF* __restrict__ kv = SolF::kp(d.kf, st.kperm, i);
-                        CF x[RC];
-#pragma unroll
-                        for (int c = 0; c < RC; c++) x[c] = kv[SolF::bin(s0 + c)];
-#pragma unroll
-                        for (int c = 0; c < RC; c++)
-#pragma unroll
-                            for (int q = 0; q < 4; q++) {
-                                cr[c][q] += kT5r[i][q] * (double)x[c].re;
-                                ci[c][q] += kT5r[i][q] * (double)x[c].im;
-                            }
-                    }
-#pragma unroll
-                    for (int c = 0; c < RC; c++) {
-                        const int b = SolF::bin(s0 + c);
-                        sg[b] = down<RF>(ld2(u, b));
-#pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            sg[(q + 1) * N + b] = mk((RF)cr[c][q], (RF)ci[c][q]);
-                    }
-                }
+                    store_interp<RF, LOGN, LOGE>(d, u, st.kperm,
+                                                 (CF*)d.seg + (size_t)(n - sb.lo) * 5 * N);
                 st.cur ^= 1;
                 st.kperm ^= 1;
                 st.rec_pos++;
+                st.nrec++;
                 if (n + 1 >= sb.hi) st.phase = st.a_nf == 0 ? PH_ADJ_INIT : PH_ADJ;
                 continue;
             }
@@ -1053,6 +1081,11 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     d.steplog[2 * st.nsteps] = z;
                     d.steplog[2 * st.nsteps + 1] = dt;
                 }
+                // while the solve fits the interpolant buffer, keep each
+                // step's interpolant now: the adjoint then needs no recompute
+                if (st.nsteps < d.seg_cap)
+                    store_interp<RF, LOGN, LOGE>(d, u, st.kperm,
+                                                 (CF*)d.seg + (size_t)st.nsteps * 5 * N);
             }
             double znew = z + dt;
             if (fabs(znew - L) < 100.0 * kEps * fmax(z, L)) znew = L;  // snap to the tstop

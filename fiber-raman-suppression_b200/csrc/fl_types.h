@@ -102,6 +102,8 @@ struct SlotState {
     long naccept, nreject, nf;
     long a_naccept, a_nreject, a_nf;
     long iters, a_iters;
+    long nrec;               // forward steps recomputed for the adjoint
+    int dense;               // the forward kept every step's interpolant: no recompute
 };
 
 // ---------------------------------------------------------------------------
@@ -179,6 +181,8 @@ struct MmState {
     long naccept, nreject, nf;
     long a_naccept, a_nreject, a_nf;
     long iters, a_iters;
+    long nrec;              // forward steps recomputed for the adjoint
+    int dense;              // always 0: the multimode forward keeps checkpoints only
 };
 
 // ---------------------------------------------------------------------------

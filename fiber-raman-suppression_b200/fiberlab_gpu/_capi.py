@@ -29,7 +29,8 @@ EXPORTS = ("fl_version", "fl_status_string", "fl_ctx_create", "fl_ctx_destroy",
            "fl_mode_phase_gradient_batch_device", "fl_server_create", "fl_server_destroy",
            "fl_server_submit", "fl_server_poll", "fl_server_wait", "fl_server_info_get",
            "fl_problem_set_objective", "fl_forward_gain", "fl_ctx_set_stream",
-           "fl_ctx_get_stream", "fl_forward_times")
+           "fl_ctx_get_stream", "fl_forward_times",
+           "fl_forward_evidence")
 
 # device objectives (FL_OBJ_*) by the reference's objective names
 # (physics_models.jl:947-962); temporal_width runs with a host seed
@@ -55,7 +56,7 @@ class FlStats(C.Structure):
     _fields_ = [("naccept", C.c_long), ("nreject", C.c_long), ("nf", C.c_long),
                 ("adj_naccept", C.c_long), ("adj_nreject", C.c_long), ("adj_nf", C.c_long),
                 ("status", C.c_int), ("checkpoints_used", C.c_int), ("J", C.c_double),
-                ("z_end", C.c_double)]
+                ("z_end", C.c_double), ("recompute_steps", C.c_long)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -127,6 +128,7 @@ def load() -> C.CDLL:
         lib.fl_mode_phase_gradient_batch_device.argtypes = [vp, vp, ip, vp, vp, ip, vp, vp, vp]
         lib.fl_rhs_eval.argtypes = [vp, ip, dp, vp, vp, vp]
         lib.fl_forward_times.argtypes = [vp, vp, C.c_long, C.POINTER(C.c_long)]
+        lib.fl_forward_evidence.argtypes = [vp, ip, vp]
         lib.fl_ctx_timing.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.fl_server_create.argtypes = [vp, C.POINTER(FlServerOpts), C.POINTER(vp)]
         lib.fl_server_destroy.argtypes = [vp]
@@ -161,7 +163,7 @@ def forward_noalloc(device: int, nt: int, d_D: int, gamma: float, d_hR: int, d_s
 class Context:
     """fl_ctx on one device (one per host thread)."""
 
-    def __init__(self, device: int = 0, checkpoints: int = 32, segment_steps: int = 16,
+    def __init__(self, device: int = 0, checkpoints: int = 32, segment_steps: int = 64,
                  step_log: int = 0, max_iters: int = 100000, hbm_budget_bytes: int = 0):
         lib = load()
         self.opts = FlCtxOpts(hbm_budget_bytes, checkpoints, segment_steps, step_log, max_iters)
@@ -292,6 +294,15 @@ class GPUProblem:
         t = np.empty(n.value)
         self.ctx.check(load().fl_forward_times(self.h, _ptr(t), n.value, C.byref(n)))
         return t
+
+    def forward_evidence(self, nsave: int) -> np.ndarray:
+        """Device FP64 evidence sums of the last forward's nsave saved
+        spectra (fl_forward_evidence): rows of [Σ P(t), max P(t), P at the
+        temporal edges, Σ S(ω), S at the spectral edges, Σ |u|²/|selfsteep|,
+        then Σ_t |fft(u_m)|² per mode]."""
+        ev = np.empty((int(nsave), 6 + self.fp.M))
+        self.ctx.check(load().fl_forward_evidence(self.h, int(nsave), _ptr(ev)))
+        return ev
 
     def adjoint(self, lambdaL):
         lam = np.ascontiguousarray(lambdaL, dtype=np.complex128)

@@ -178,6 +178,8 @@ class PropagationResult:
     accepted_steps: int
     rhs_evaluations: int
     problem: Optional[P.FiberProblem] = None
+    # per save position, the device's FP64 evidence sums (fl_forward_evidence)
+    device_evidence: Optional[np.ndarray] = None
 
 
 def save_positions(saveat, length_m: float) -> np.ndarray:
@@ -208,12 +210,15 @@ def propagate(fp: P.FiberProblem, saveat=None, *, precision="fp32",
     return PropagationResult(z_m=z, spectra=spectra, input_spectrum=spectra[0].copy(),
                              output_spectrum=spectra[-1].copy(),
                              accepted_steps=stats["naccept"], rhs_evaluations=stats["nf"],
-                             problem=fp)
+                             problem=fp, device_evidence=gp.forward_evidence(len(z)))
 
 
 # ---------------------------------------------------------------------------
-# Evidence over the saved spectra (propagation.jl:176-304): FP64 reductions
-# of the lab-frame samples the GPU forward returned.
+# Evidence over the saved spectra (propagation.jl:176-304).  A GPU result
+# carries the FP64 reductions the device ran over its saved spectra
+# (fl_forward_evidence, device_field_metrics); field_metrics restates the
+# same reductions on the host for results made elsewhere (and checks the
+# device sums in the tests).
 
 def edge_fraction(power: np.ndarray) -> float:
     """_edge_fraction (propagation.jl:176-182): power in the first and last
@@ -241,6 +246,19 @@ def field_metrics(spectrum: np.ndarray, sim: dict) -> dict:
             "photon_number": P.photon_number(u, sim)}
 
 
+def device_field_metrics(ev: np.ndarray, sim: dict) -> dict:
+    """field_metrics of one save position from the device's FP64 sums
+    (fl_forward_evidence): the reductions ran on the GPU; only the grid
+    constants Δt and ω0 are applied here."""
+    dt = float(sim["Δt"])
+    mode_energy = np.asarray(ev[6:], dtype=np.float64) * dt
+    return {"energy_pj": float(ev[0] * dt), "mode_energy_pj": mode_energy,
+            "peak_power_w": float(ev[1]),
+            "temporal_edge_fraction": float(ev[2] / ev[0]),
+            "spectral_edge_fraction": float(ev[4] / ev[3]),
+            "photon_number": float(ev[5] * dt / float(sim["ω0"]))}
+
+
 def _integrity(result: PropagationResult) -> bool:
     """The structural part of _propagation_integrity (propagation.jl:125-145):
     sizes, ordered finite positions from 0 to L, and the input/output samples
@@ -265,7 +283,11 @@ def _integrity(result: PropagationResult) -> bool:
 def _propagation_metrics(result: PropagationResult) -> dict:
     """_propagation_metrics (propagation.jl:204-237)."""
     fp = result.problem
-    samples = [field_metrics(result.spectra[i], fp.sim) for i in range(len(result.z_m))]
+    ev = result.device_evidence
+    if ev is not None and np.shape(ev) == (len(result.z_m), 6 + fp.M):
+        samples = [device_field_metrics(ev[i], fp.sim) for i in range(len(result.z_m))]
+    else:  # a result that did not come from the GPU (no device sums)
+        samples = [field_metrics(result.spectra[i], fp.sim) for i in range(len(result.z_m))]
     inp, out = samples[0], samples[-1]
     energy_drift = np.array([s["energy_pj"] / inp["energy_pj"] - 1 for s in samples])
     photon_drift = np.array([s["photon_number"] / inp["photon_number"] - 1 for s in samples])

@@ -60,10 +60,13 @@ typedef struct fl_server fl_server;
 typedef struct {
     size_t hbm_budget_bytes;   /* 0: no limit beyond cudaMalloc */
     int checkpoints;           /* z-checkpoint slots K for the adjoint (power of 2, default 32) */
-    int segment_steps;         /* dense-output steps kept per recompute sub-segment (default 16):
-                                  a solve of more than K x segment_steps accepted steps replays
-                                  each checkpoint segment once per sub-segment instead of
-                                  failing, so K and segment_steps trade memory for recompute */
+    int segment_steps;         /* dense-output steps kept (default 64).  A solve of at most
+                                  segment_steps accepted steps keeps every step's interpolant
+                                  during the forward and its adjoint recomputes nothing;
+                                  longer solves recompute from the K checkpoints, replaying
+                                  each checkpoint segment once per sub-segment of
+                                  segment_steps steps (never failing for capacity), so K and
+                                  segment_steps trade memory for recompute */
     int step_log;              /* accepted-step log capacity; 0 (default): max_iters entries,
                                   so the log never ends a solve the step limit admits */
     long max_iters;            /* attempted steps per integration (default 100000, as maxiters) */
@@ -78,6 +81,8 @@ typedef struct {
     int checkpoints_used;
     double J;          /* objective value (band gradient calls) */
     double z_end;
+    long recompute_steps;  /* forward steps recomputed by the adjoint from checkpoints
+                              (0 when the forward kept every step's interpolant) */
 } fl_stats;
 
 /* Library version string and status names. */
@@ -223,6 +228,25 @@ int fl_mode_phase_gradient_batch(fl_problem *prob, const double *u0, int nbatch,
  * first min(cap, *n_out) are written to t_out (cap 0 only queries the
  * count).  FL_EINVAL without a completed preceding fl_forward. */
 int fl_forward_times(fl_problem *prob, double *t_out, long cap, long *n_out);
+
+/* Evidence of the last fl_forward (which must have had nsave save
+ * positions): FP64 reductions of each saved lab-frame spectrum u on the
+ * device, the sums behind propagate's metrics and verify
+ * (src/fiberlab/propagation.jl:176-237).  ev_out receives nsave rows of
+ * 6 + M values:
+ *   [0] Σ_t P(t), P(t) = Σ_m |fft(u_m)(t)|² (the temporal power; times Δt:
+ *       the energy in pJ)
+ *   [1] max_t P(t) (the peak power in W)
+ *   [2] P summed over the first and last max(1, floor(0.05 Nt)) samples
+ *       ([2]/[0]: the temporal edge fraction)
+ *   [3] Σ_ω S(ω), S = Σ_m |u_m(ω)|² (the spectral power)
+ *   [4] S summed over the same edges of fftshift(S) ([4]/[3]: the spectral
+ *       edge fraction)
+ *   [5] Σ |u|² / |selfsteep| (times Δt/ω0: the photon number, with
+ *       selfsteep = fftshift(ωs/ω0) as given to fl_problem_create)
+ *   [6 + m] Σ_t |fft(u_m)(t)|² (times Δt: mode m's energy in pJ)
+ * FL_EINVAL without such a forward. */
+int fl_forward_evidence(fl_problem *prob, int nsave, double *ev_out);
 
 /* One evaluation of the forward right-hand side disp_mmf!
  * (simulate_disp_mmf.jl:25-60) or, with adjoint = 1, of adjoint_disp_mmf!

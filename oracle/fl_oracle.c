@@ -47,29 +47,16 @@ typedef double complex cplx;
 
 typedef struct {
     int n;
-    int *rev;
-    cplx *tw; /* exp(-2 pi i k / n), k < n/2 */
+    cplx *tw;   /* exp(-2 pi i k / n), k < n */
+    cplx *work; /* n values of scratch (one plan per thread) */
 } fft_plan;
-
-static int ilog2(int n) {
-    int l = 0;
-    while ((1 << l) < n) l++;
-    return l;
-}
 
 static int plan_init(fft_plan *pl, int n) {
     pl->n = n;
-    pl->rev = (int *)malloc(sizeof(int) * (size_t)n);
-    pl->tw = (cplx *)malloc(sizeof(cplx) * (size_t)(n / 2 > 0 ? n / 2 : 1));
-    if (!pl->rev || !pl->tw) return -1;
-    int lg = ilog2(n);
-    for (int i = 0; i < n; i++) {
-        int r = 0;
-        for (int b = 0; b < lg; b++)
-            if (i & (1 << b)) r |= 1 << (lg - 1 - b);
-        pl->rev[i] = r;
-    }
-    for (int k = 0; k < n / 2; k++) {
+    pl->tw = (cplx *)malloc(sizeof(cplx) * (size_t)n);
+    pl->work = (cplx *)malloc(sizeof(cplx) * (size_t)n);
+    if (!pl->tw || !pl->work) return -1;
+    for (int k = 0; k < n; k++) {
         double a = -2.0 * M_PI * (double)k / (double)n;
         pl->tw[k] = cos(a) + I * sin(a);
     }
@@ -77,38 +64,64 @@ static int plan_init(fft_plan *pl, int n) {
 }
 
 static void plan_free(fft_plan *pl) {
-    free(pl->rev);
     free(pl->tw);
-    pl->rev = NULL;
+    free(pl->work);
     pl->tw = NULL;
+    pl->work = NULL;
 }
 
+static inline cplx cmul_(cplx a, cplx b) {
+    return CMPLX(creal(a) * creal(b) - cimag(a) * cimag(b),
+                 creal(a) * cimag(b) + cimag(a) * creal(b));
+}
+
+/* Radix-4 Stockham autosort pass (decimation in frequency) over
+ * sub-sequences of length n at stride s, reading x and writing y, then the
+ * rest of the transform on y; a final radix-2 pass when log2 n is odd.  eo
+ * tracks which buffer must hold the result, so it ends in the caller's
+ * array.  tw is the length-nfull table exp(-2 pi i k / nfull). */
+static void stockham(int n, int s, int eo, cplx *x, cplx *y, const cplx *tw, int nfull) {
+    if (n == 1) {
+        if (eo)
+            for (int q = 0; q < s; q++) y[q] = x[q];
+        return;
+    }
+    if (n == 2) {
+        cplx *z = eo ? y : x;
+        for (int q = 0; q < s; q++) {
+            const cplx a = x[q], b = x[q + s];
+            z[q] = a + b;
+            z[q + s] = a - b;
+        }
+        return;
+    }
+    const int n1 = n / 4, n2 = n / 2, n3 = n1 + n2, st = nfull / n;
+    for (int p = 0; p < n1; p++) {
+        const cplx w1 = tw[p * st], w2 = tw[2 * p * st], w3 = tw[3 * p * st];
+        for (int q = 0; q < s; q++) {
+            const cplx a = x[q + s * p], b = x[q + s * (p + n1)];
+            const cplx c = x[q + s * (p + n2)], d = x[q + s * (p + n3)];
+            const cplx apc = a + c, amc = a - c, bpd = b + d, bmd = b - d;
+            const cplx jbmd = CMPLX(-cimag(bmd), creal(bmd)); /* i (b - d) */
+            y[q + s * (4 * p + 0)] = apc + bpd;
+            y[q + s * (4 * p + 1)] = cmul_(w1, amc - jbmd);
+            y[q + s * (4 * p + 2)] = cmul_(w2, apc - bpd);
+            y[q + s * (4 * p + 3)] = cmul_(w3, amc + jbmd);
+        }
+    }
+    stockham(n1, 4 * s, !eo, y, x, tw, nfull);
+}
+
+/* unnormalised forward transform (exponent -1); the inverse is
+ * conj(F(conj x)) / n (FFTW's conventions as used by the reference) */
 static void fft_1d(const fft_plan *pl, cplx *a, int inverse) {
-    int n = pl->n;
-    for (int i = 0; i < n; i++) {
-        int r = pl->rev[i];
-        if (r > i) {
-            cplx t = a[i];
-            a[i] = a[r];
-            a[r] = t;
-        }
-    }
-    for (int len = 2; len <= n; len <<= 1) {
-        int half = len >> 1, step = n / len;
-        for (int i = 0; i < n; i += len) {
-            for (int j = 0; j < half; j++) {
-                cplx w = pl->tw[j * step];
-                if (inverse) w = conj(w);
-                cplx u = a[i + j];
-                cplx v = a[i + j + half] * w;
-                a[i + j] = u + v;
-                a[i + j + half] = u - v;
-            }
-        }
-    }
+    const int n = pl->n;
+    if (inverse)
+        for (int i = 0; i < n; i++) a[i] = conj(a[i]);
+    stockham(n, 1, 0, a, pl->work, pl->tw, n);
     if (inverse) {
-        double s = 1.0 / (double)n;
-        for (int i = 0; i < n; i++) a[i] *= s;
+        const double sc = 1.0 / (double)n;
+        for (int i = 0; i < n; i++) a[i] = CMPLX(creal(a[i]) * sc, -cimag(a[i]) * sc);
     }
 }
 

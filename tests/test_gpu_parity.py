@@ -403,6 +403,54 @@ def test_propagate_metrics_and_verify(gpu_ctx):
         assert not S.verify(res, min_launch_samples_per_fwhm=16)["pass"]
 
 
+@pytest.mark.parametrize("shape", ["sm1024", "sm16384", "sm32768", "mm3x512"])
+def test_device_evidence_matches_host_reductions(gpu_ctx, shape):
+    # fl_forward_evidence: the FP64 reductions behind metrics/verify run on
+    # the device over the saved spectra (one CTA per save position, a 4-CTA
+    # cluster at 2^15); the host restatement of propagation.jl:176-202 over
+    # the same spectra is the check
+    from fiberlab_gpu import solve as S
+    if shape.startswith("sm"):
+        nt = int(shape[2:])
+        fp = P.single_mode_problem(nt=nt, time_window_ps=10.0, L=0.2, power_w=0.1,
+                                   rep_rate_hz=80e6, validate_grid=False)
+    else:
+        fp = P.multimode_problem(1, 32, 512, 5.0, 0.3, 4e-9, 200e-15, seed=1,
+                                 raman_threshold_thz=-5.0)
+    zs = [0.0, 0.37 * fp.L, fp.L]
+    res = S.propagate(fp, zs, ctx=gpu_ctx)
+    assert res.device_evidence.shape == (3, 6 + fp.M)
+    for i in range(3):
+        dev = S.device_field_metrics(res.device_evidence[i], fp.sim)
+        host = S.field_metrics(res.spectra[i], fp.sim)
+        for key in ("energy_pj", "peak_power_w", "photon_number"):
+            assert dev[key] == pytest.approx(host[key], rel=1e-12), key
+        np.testing.assert_allclose(dev["mode_energy_pj"], host["mode_energy_pj"], rtol=1e-12)
+        for key in ("temporal_edge_fraction", "spectral_edge_fraction"):
+            assert dev[key] == pytest.approx(host[key], rel=1e-9, abs=1e-18), key
+    # metrics from the device sums and from the host reductions agree
+    host_res = S.PropagationResult(**{**res.__dict__, "device_evidence": None})
+    a, b = S.metrics(res), S.metrics(host_res)
+    for key in ("max_photon_number_drift", "max_temporal_edge_fraction", "output_energy_pj"):
+        assert a[key] == pytest.approx(b[key], rel=1e-9, abs=1e-12), key
+
+
+def test_dense_forward_adjoint_needs_no_recompute(gpu_ctx):
+    # a solve of at most segment_steps accepted steps keeps every step's
+    # interpolant during the forward: its adjoint recomputes nothing and
+    # integrates 0 <- L without checkpoint stops; a small segment buffer
+    # forces the checkpoint recompute; both match the oracle
+    fp = cfg0(raman_threshold_thz=-13.0)
+    phi = 0.5 * np.random.default_rng(0).standard_normal(fp.nt)
+    Jd, gd, sd = GPUProblem(Context(0, segment_steps=64), fp).phase_gradient_batch(phi[None, :])
+    Jr, gr, sr = GPUProblem(Context(0, segment_steps=4), fp).phase_gradient_batch(phi[None, :])
+    assert sd[0]["recompute_steps"] == 0 and sd[0]["naccept"] <= 64
+    assert sr[0]["recompute_steps"] >= sr[0]["naccept"]
+    assert Jd[0] == Jr[0]                     # the same forward solve
+    Jo, go, _ = O.phase_gradient(fp, phi)
+    assert rel(gd[0], go) < GRAD_TOL and rel(gr[0], go) < GRAD_TOL
+
+
 def test_lbfgs_batched_inverse_design(gpu_ctx):
     # optimize_spectral_phase (raman_optimization.jl:183-246) for two starts
     # in lockstep: every line search is one batched forward + adjoint launch
