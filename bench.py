@@ -39,6 +39,7 @@ UNIT = "solves/s"
 NT, T_PS, L_M, P_W, REP = 8192, 10.0, 0.5, 0.1, 80e6
 BYTES_FWD_STEP = 336  # per point per attempted forward step (FP32 complex field passes)
 BYTES_ADJ_STEP = 384  # per point per attempted adjoint step
+ORACLE_FFT = "radix-4 Stockham FP64 FFT in C, x86-64-v3 build (FFTW is not available)"
 
 
 def workload_problem():
@@ -53,12 +54,24 @@ def phases(rank: int, B: int, nt: int) -> np.ndarray:
     return 0.5 * rng.standard_normal((B, nt))
 
 
-def config(B, world, extra=None):
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def config(B, world, extra=None,
+           precision="FP32 bulk; FP64 phase/state/error norm/reductions; FP64 adjoint"):
     c = {"workload": f"single-mode inverse-design batch: Nt=2^13 over 10 ps, SMF-28, L=0.5 m, "
                      f"0.1 W/80 MHz 185 fs sech², phase N(0,0.5²), Raman band < -13 THz, "
-                     f"fwd+adjoint with 32 z-checkpoints",
+                     f"fwd+adjoint, 32 z-checkpoints / 64 dense-output steps",
          "batch_per_gpu": B, "global_batch": B * world, "nt": NT, "modes": 1,
-         "precision": "FP32 bulk; FP64 phase/error norm/reductions/gradient",
+         "precision": precision,
          "parallelism": f"replicas x{world}", "l2": "inputs and per-slot workspaces > L2 (126 MB)"}
     if extra:
         c.update(extra)
@@ -140,16 +153,73 @@ def cpu_baseline(fp, nthreads: int, nprob: int):
     return nprob / dt, dt
 
 
-def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3, window_s=0.0):
-    """Config-3 stream: n requests with Poisson arrivals at 2000/s, log2 Nt
+SERVE_MIX = ("config 3: Poisson 2000/s, Nt 2^11..2^15 over 10 ps, L U(0.1,5) m, P U(0.02,0.3) W, "
+             "half fwd / half fwd+adjoint (phase N(0,0.5^2)), FP32, seed 3")
+
+
+def _quantiles(lat):
+    return ({"latency_ms_p50": float(np.percentile(lat, 50)),
+             "latency_ms_p99": float(np.percentile(lat, 99))} if lat else
+            {"latency_ms_p50": None, "latency_ms_p99": None})
+
+
+def _plain_worker(q, stop, dev_index, n, seed, window_s):
+    """The plain one-at-a-time drop-in over the config-3 stream, in a child
+    process: request i starts when it has arrived and request i-1 has
+    finished, through the plain entry points with a problem per request
+    (the reference builds its tables per solve).  Reports each completion
+    (time since the stream's start, latency from arrival); stops starting
+    requests when asked or after the window."""
+    for _p in (ROOT, PKG):
+        if _p not in sys.path:
+            sys.path.insert(0, _p)
+    from fiberlab_gpu import problem as P
+    from fiberlab_gpu._capi import Context, FiberLabGPUError, GPUProblem
+    reqs = P.serving_mix(n, seed=seed)
+    grids = {nt: P.serving_grid_problem(nt) for nt in sorted({r.nt for r in reqs})}
+    ctx = Context(dev_index, checkpoints=256, segment_steps=128, max_iters=400000)
+    # one small solve per grid outside the stream (module load, first launches)
+    for fp0 in grids.values():
+        fp = P.FiberProblem(**{**fp0.__dict__})
+        fp.L = 1e-3
+        GPUProblem(ctx, fp).forward(P.serving_launch(fp0, 0.02))
+    q.put(("start",))
+    t0 = time.perf_counter()
+    for i, r in enumerate(reqs):
+        now = time.perf_counter() - t0
+        if stop.is_set() or now > window_s:
+            break
+        if now < r.arrival_s:
+            time.sleep(r.arrival_s - now)
+        fp0 = grids[r.nt]
+        u0 = P.serving_launch(fp0, r.power_w)
+        status = 0
+        try:
+            fp = P.FiberProblem(**{**fp0.__dict__})
+            fp.L = r.L
+            gp = GPUProblem(ctx, fp)
+            if r.kind == 0:
+                gp.forward(u0)
+            else:
+                gp.phase_gradient_batch(r.phase[None, :], u0=u0)
+        except FiberLabGPUError as e:
+            status = e.status
+        fin = time.perf_counter() - t0
+        q.put(("done", i, status, fin, fin - r.arrival_s))
+    q.put(("end",))
+
+
+def serving_measure(ctx_cls, dev_index, n, window_s, plain_window_s, seed=3):
+    """Config-3 stream (n requests, Poisson arrivals at 2000/s, log2 Nt
     uniform on 11..15 over 10 ps, L ~ U(0.1, 5) m, P ~ U(0.02, 0.3) W, half
-    forward-only and half forward + band gradient with phase N(0, 0.5²),
-    through the continuous-batching server; then the first plain_n requests
-    of the same stream one at a time through the plain entry points (a
-    problem per request, as the reference builds its tables per solve).
-    With window_s > 0 both paths instead take the stream in arrival order for
-    window_s seconds and count the requests completed in that time (the
-    server's in-flight remainder is then abandoned)."""
+    forward-only and half forward + band gradient with phase N(0, 0.5²)),
+    taken by both paths in arrival order over a bounded window: the
+    continuous-batching server (requests submitted as they arrive) for
+    window_s seconds, then the plain one-at-a-time path for plain_window_s
+    seconds.  Each path reports the requests completed inside its window,
+    solves/s, p50/p99 latency (arrival to result) of those, the requests
+    arrived but unfinished at the window's end and failures by status."""
+    import multiprocessing as mp
     from fiberlab_gpu import problem as P
     from fiberlab_gpu._capi import FiberLabGPUError, GPUProblem
     from fiberlab_gpu.serving import Server
@@ -164,12 +234,12 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3, window_s=0.0):
     # allocate each shape's first chunk outside the measured stream
     for nt, (fp, gp) in sorted(grids.items()):
         srv.wait(srv.submit_forward(gp, u0=P.serving_launch(fp, 0.02), L=1e-3))
-    handles, statuses, lat = [], {}, []
+    statuses, lat = {}, []
     t0 = time.perf_counter()
-    i, outstanding, t_last = 0, [], t0
-    while i < n or outstanding:
+    i, outstanding = 0, []
+    while True:
         now = time.perf_counter() - t0
-        if window_s and now > window_s:
+        if now > window_s or (i >= n and not outstanding):
             break
         while i < n and reqs[i].arrival_s <= now:
             r = reqs[i]
@@ -189,56 +259,61 @@ def serving_measure(ctx_cls, dev_index, n, plain_n, seed=3, window_s=0.0):
                 lat.append(h.latency_ms)
             except FiberLabGPUError as e:
                 statuses[e.status] = statuses.get(e.status, 0) + 1
-            t_last = time.perf_counter()
         outstanding = still
         time.sleep(0.0005)
-    wall = window_s if window_s else t_last - t0
+    wall = min(time.perf_counter() - t0, window_s)
     info = srv.info()
     srv.close()
     done = statuses.get(0, 0)
-    out = {"requests": n, "completed": done,
-           "failed_by_status": {str(k): v for k, v in statuses.items() if k != 0},
-           "solves_per_s": done / wall, "wall_s": wall,
-           "latency_ms_p50": float(np.percentile(lat, 50)) if lat else None,
-           "latency_ms_p99": float(np.percentile(lat, 99)) if lat else None,
-           "slots": info["slots"], "hbm_bytes": info["hbm_bytes"],
-           "mix": "config 3: Poisson 2000/s, Nt 2^11..2^15 over 10 ps, L U(0.1,5) m, "
-                  "P U(0.02,0.3) W, half fwd / half fwd+adjoint (phase N(0,0.5^2)), FP32, seed 3"}
-    # plain one-at-a-time drop-in on the first plain_n requests of the stream
-    pctx = ctx_cls(dev_index, checkpoints=256, segment_steps=128, step_log=32768,
-                   max_iters=400000)
-    tp, pdone = 0.0, 0
-    for r in (reqs if window_s else reqs[:plain_n]):
-        if window_s and tp > window_s:
-            break
-        fp0, _ = grids[r.nt]
-        u0 = P.serving_launch(fp0, r.power_w)
-        t = time.perf_counter()
-        ok = False
+    served = {"window_s": window_s, "completed": done, "solves_per_s": done / wall,
+              **_quantiles(lat), "unfinished": i - sum(statuses.values()),
+              "failed_by_status": {str(k): v for k, v in statuses.items() if k != 0},
+              "slots": info["slots"], "hbm_bytes": info["hbm_bytes"]}
+
+    # the plain path in a child process, stopped between requests at the
+    # window's end (a request still running then is waited for, up to a bound)
+    mpc = mp.get_context("spawn")
+    q, stop = mpc.Queue(), mpc.Event()
+    child = mpc.Process(target=_plain_worker, args=(q, stop, dev_index, n, seed, plain_window_s),
+                        daemon=True)
+    child.start()
+    pst, plat = {}, []
+    try:
+        q.get(timeout=600)                         # the child's "start"
+        ended = False
+    except Exception:
+        ended = True                               # the child did not start: no plain number
+    t_start = time.perf_counter()
+    while not ended:
+        left = plain_window_s - (time.perf_counter() - t_start)
+        if left <= 0 and not stop.is_set():
+            stop.set()
         try:
-            fp = P.FiberProblem(**{**fp0.__dict__})
-            fp.L = r.L
-            gp = GPUProblem(pctx, fp)
-            if r.kind == 0:
-                gp.forward(u0)
-            else:
-                gp.phase_gradient_batch(r.phase[None, :], u0=u0)
-            ok = True
-        except FiberLabGPUError:
-            pass
-        tp += time.perf_counter() - t
-        if ok and not (window_s and tp > window_s):  # finished inside the window
-            pdone += 1
-    if window_s:
-        out["window_s"] = window_s
-        out["plain_one_at_a_time"] = {"completed_in_window": pdone,
-                                      "solves_per_s": pdone / window_s}
-    else:
-        out["plain_one_at_a_time"] = {"requests": plain_n, "completed": pdone,
-                                      "solves_per_s": plain_n / tp, "total_s": tp}
-    ps = out["plain_one_at_a_time"]["solves_per_s"]
-    out["speedup_vs_plain"] = out["solves_per_s"] / ps if ps > 0 else None
-    return out
+            msg = q.get(timeout=max(0.05, min(left, 1.0)) if left > 0 else 120.0)
+        except Exception:
+            break                                  # a request outlived the grace period
+        if msg[0] == "end":
+            ended = True
+        elif msg[0] == "done":
+            _, idx, status, fin, latency = msg
+            if fin <= plain_window_s:
+                pst[status] = pst.get(status, 0) + 1
+                if status == 0:
+                    plat.append(1e3 * latency)
+    if child.is_alive():
+        child.join(timeout=5)
+    if child.is_alive():
+        child.terminate()
+        child.join(timeout=30)
+    arrived = sum(1 for r in reqs if r.arrival_s <= plain_window_s)
+    pdone = pst.get(0, 0)
+    plain = {"window_s": plain_window_s, "completed": pdone,
+             "solves_per_s": pdone / plain_window_s, **_quantiles(plat),
+             "unfinished": arrived - sum(pst.values()),
+             "failed_by_status": {str(k): v for k, v in pst.items() if k != 0}}
+    return {"requests": n, "mix": SERVE_MIX, "served": served, "plain_one_at_a_time": plain,
+            "served_over_plain": (served["solves_per_s"] / plain["solves_per_s"]
+                                  if plain["solves_per_s"] > 0 else None)}
 
 
 def optimizer_measure(ctx, B, probes, iters):
@@ -283,10 +358,13 @@ def multimode_measure(ctx, dev, B, steps, warmup):
     Nt = 2^12 over 5 ps, 1 m, 2 nJ), one forward + adjoint."""
     import torch
     from fiberlab_gpu import problem as P
-    from fiberlab_gpu._capi import GPUProblem
+    from fiberlab_gpu._capi import Context, GPUProblem
     out = {}
     fp = P.multimode_problem(3, 96, 16384, 10.0, 2.0, 5e-9, 200e-15, seed=0,
                              raman_threshold_thz=-2.0)
+    # the multimode forward keeps checkpoints only: a 16-step recompute
+    # buffer per slot is enough for 32 checkpoints of these solves
+    ctx = Context(ctx.device, checkpoints=32, segment_steps=16)
     gp = GPUProblem(ctx, fp)
     ph = np.random.default_rng(4).standard_normal((B, fp.M, fp.nt))
     d_u0 = torch.from_numpy(np.ascontiguousarray(fp.uw0).view(np.float64).copy()).to(dev)
@@ -303,13 +381,30 @@ def multimode_measure(ctx, dev, B, steps, warmup):
     for _ in range(steps):
         st = run()
         ms.append(ctx.timing()[0])
+    M, N = fp.M, fp.nt
+    fwd_att = sum(s["naccept"] + s["nreject"] for s in st)
+    rec = sum(s["recompute_steps"] for s in st)
+    adj_att = sum(s["adj_naccept"] + s["adj_nreject"] for s in st)
+    t_batch = float(np.mean(ms)) / 1e3
+    # roofline bytes per attempted step: 336 N M (forward and recompute), 384 N M (adjoint)
+    alg_bytes = (BYTES_FWD_STEP * (fwd_att + rec) + BYTES_ADJ_STEP * adj_att) * N * M
+    peak, peak_kind = measured_peak()
+    # tensor-pipe work: the FP32 forward contraction, 2 M^4 N flops per forward RHS
+    # (6 per attempted step, forward and recompute), on tcgen05 kind::tf32
+    tc_flops = 2 * M ** 4 * N * 6 * (fwd_att + rec)
     out["config4"] = {
         "workload": f"config 4: M=10 HG(m+n<=3), Nt=2^14 over 10 ps, L=2 m, 5 nJ, {B} per-mode "
-                    "phase candidates N(0,1), fwd+adjoint, checkpoints 32 x 16",
+                    "phase candidates N(0,1), fwd+adjoint, checkpoints 32 x 64",
         "solves_per_s": B * steps / (sum(ms) / 1e3), "ms_per_batch": float(np.mean(ms)),
-        "steps_per_solve": {"forward": float(np.mean([s["naccept"] + s["nreject"] for s in st])),
-                            "adjoint": float(np.mean([s["adj_naccept"] + s["adj_nreject"]
-                                                      for s in st]))},
+        "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B,
+                            "recomputed": rec / B},
+        "roofline": {"bound": "hbm", "achieved": alg_bytes / t_batch / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg_bytes / t_batch / 1e9 / peak,
+                     "peak_source": peak_kind, "alg_bytes_per_batch": alg_bytes,
+                     "scope": "whole batch (all multimode kernels) over its call time"},
+        "tensor": {"flops_per_batch": tc_flops,
+                   "achieved_tflops_over_batch": tc_flops / t_batch / 1e12,
+                   "note": "forward contraction only; 3 tf32 MMAs per product (3xTF32 split)"},
         "contraction": "tcgen05 kind::tf32 (3xTF32) for the FP32 forward, DFMA for the adjoint"}
     fp2 = P.multimode_problem(2, 64, 4096, 5.0, 1.0, 2e-9, 200e-15, seed=0,
                               raman_threshold_thz=-2.0)
@@ -367,9 +462,11 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": config(nprob, 1, {"implementation": "FP64 C restatement of the reference "
                                         "Julia solver (Julia is not installed), OpenMP over "
-                                        "independent problems"}),
+                                        "independent problems"},
+                             precision="FP64 throughout"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                             "sample": sample},
+                             "sample": sample, "cpu_model": cpu_model(),
+                             "fft": ORACLE_FFT},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -387,7 +484,7 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    ctx = Context(local, checkpoints=32, segment_steps=16)
+    ctx = Context(local, checkpoints=32, segment_steps=64)
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     B = args.batch or 4 * sms
     fp = workload_problem()
@@ -432,7 +529,7 @@ def run_ours(args):
     # roofline of the stepper kernel: algorithmic bytes per launch / launch time
     st = stats_all[-1]
     fwd_att = sum(s["naccept"] + s["nreject"] for s in st)
-    rec = sum(s["naccept"] for s in st)
+    rec = sum(s["recompute_steps"] for s in st)   # forward steps the adjoint recomputed
     adj_att = sum(s["adj_naccept"] + s["adj_nreject"] for s in st)
     alg_bytes = (BYTES_FWD_STEP * (fwd_att + rec) + BYTES_ADJ_STEP * adj_att) * fp.nt
     peak, peak_kind = measured_peak()
@@ -450,7 +547,9 @@ def run_ours(args):
     gp.phase_gradient_batch(pin_ph.numpy(), fp.mask, fp.uw0,
                             out=(pin_J.numpy(), pin_g.numpy()))   # warm-up (staging area)
     e2e_t = []
-    for _ in range(max(2, min(args.steps, 3))):
+    for _ in range(args.steps):
+        flush.zero_()                      # L2 flush between timed iterations (not timed)
+        torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         gp.phase_gradient_batch(pin_ph.numpy(), fp.mask, fp.uw0,
                                 out=(pin_J.numpy(), pin_g.numpy()))
@@ -476,7 +575,8 @@ def run_ours(args):
         cores = os.cpu_count() or 1
         v, dt = cpu_baseline(fp, cores, cores)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{cores} problems of this workload, one per thread ({dt:.1f} s)"}
+               "sample": f"{cores} problems of this workload, one per thread ({dt:.1f} s)",
+               "cpu_model": cpu_model(), "fft": ORACLE_FFT}
 
     multimode = None
     if args.mm_batch and rank == 0 and world == 1:
@@ -487,9 +587,9 @@ def run_ours(args):
         optimizer = optimizer_measure(ctx, args.opt_batch, args.opt_probes, args.opt_iters)
 
     serving = None
-    if args.serve and rank == 0:
-        serving = serving_measure(Context, local, args.serve, args.serve_plain,
-                                  window_s=args.serve_window)
+    if args.serve and rank == 0 and world == 1:
+        serving = serving_measure(Context, local, args.serve, args.serve_window,
+                                  args.serve_plain_window)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -506,7 +606,8 @@ def run_ours(args):
                              "alg_bytes_per_launch": alg_bytes},
                 "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
                 "plain_one_at_a_time": plain, "batched": batched_lat,
-                "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B}}
+                "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B,
+                                    "recomputed": rec / B}}
         if multimode is not None:
             line.update(multimode)
         if optimizer is not None:
@@ -525,7 +626,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=0, help="problems per GPU (default 4 x SMs)")
-    ap.add_argument("--plain", type=int, default=8, help="one-at-a-time solves timed")
+    ap.add_argument("--plain", type=int, default=32, help="one-at-a-time solves timed")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--mm-batch", type=int, default=64,
                     help="config-4 candidates per batch reported beside the headline (0: off)")
@@ -533,12 +634,12 @@ def main():
                     help="L-BFGS optimisations run in lockstep beside the headline (0: off)")
     ap.add_argument("--opt-probes", type=int, default=4, help="trial steps per line search")
     ap.add_argument("--opt-iters", type=int, default=3, help="L-BFGS iterations timed")
-    ap.add_argument("--serve", type=int, default=0,
-                    help="also run the config-3 serving stream with this many requests")
-    ap.add_argument("--serve-window", type=float, default=0.0,
-                    help="seconds: count completions of both paths within this window")
-    ap.add_argument("--serve-plain", type=int, default=12,
-                    help="requests of that stream timed one at a time through the plain path")
+    ap.add_argument("--serve", type=int, default=4096,
+                    help="requests of the config-3 serving stream (0: off)")
+    ap.add_argument("--serve-window", type=float, default=30.0,
+                    help="seconds the server takes the stream for")
+    ap.add_argument("--serve-plain-window", type=float, default=60.0,
+                    help="seconds the plain one-at-a-time path takes the same stream for")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
