@@ -1434,6 +1434,7 @@ const char* fl_status_string(int s) {
         case FL_OOM_ADMISSION: return "request exceeds the HBM budget";
         case FL_EBUSY: return "request not finished";
         case FL_TIMEOUT: return "wait limit reached";
+        case FL_ECHECK: return "checked build: a solver index left its buffer's bounds";
         default: return "unknown status";
     }
 }

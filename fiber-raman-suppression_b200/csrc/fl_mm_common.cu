@@ -52,6 +52,13 @@ __global__ void __launch_bounds__(kMmCtl)
         c.consume();
     __syncthreads();
     c.advance();
+#ifdef FL_CHECKED
+    // the indices the next evaluation's kernels will use (checked build)
+    if (st.phase != PH_DONE && !state_in_bounds(d, st)) {
+        st.status = ST_CHECK;
+        st.phase = PH_DONE;
+    }
+#endif
     __syncthreads();
     if (threadIdx.x == 0) {
         states[slot] = st;

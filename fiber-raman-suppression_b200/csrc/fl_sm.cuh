@@ -631,6 +631,31 @@ __device__ __forceinline__ void store_interp(const SlotDesc& d, const double* u,
     }
 }
 
+// Checked build (-DFL_CHECKED): before each step of the state machine, the
+// indices a step will use -- stage, buffer parities, the step count against
+// the step log, the checkpoint segment and sub-segment against the
+// checkpoint slots and the interpolant buffer, the save position -- are
+// checked against their buffers.  A violation ends the slot with ST_CHECK
+// (FL_ECHECK) before any access, instead of trapping.  The default build
+// compiles the check away.  Shared by both steppers (SlotDesc / SlotState,
+// MmDesc / MmState).
+template <class Desc, class State>
+__device__ __forceinline__ bool state_in_bounds(const Desc& d, const State& st) {
+    bool ok = st.stage >= 0 && st.stage <= 6 && (st.cur | st.kperm | st.acur | st.akperm) >= 0 &&
+              (st.cur | st.kperm | st.acur | st.akperm) <= 1 && st.save_idx >= 0 &&
+              st.save_idx <= d.nsave && st.nsteps >= 0 &&
+              (d.step_cap == 0 || st.nsteps <= d.step_cap);
+    const int ph = st.phase;
+    if (ok && (ph == PH_REC || ph == PH_ADJ_INIT || ph == PH_ADJ)) {
+        const SubSeg sb = sub_segment(d, st);
+        ok = d.step_cap > 0 && st.nsteps >= 1 && sb.lo >= 0 && sb.lo < sb.hi &&
+             sb.hi <= st.nsteps && sb.hi - sb.lo <= d.seg_cap && st.rec_pos >= 0 &&
+             (st.dense || (st.seg >= 0 && st.seg < d.ck_cap && st.ck_stride >= 1 &&
+                           sb.seg_lo + st.rec_pos < sb.hi));
+    }
+    return ok;
+}
+
 template <typename RF, int LOGN, int LOGE>
 __device__ __forceinline__ void restore_checkpoint(const SlotDesc& d, int seg, SlotState& st) {
     using S = FftShape<LOGN, LOGE>;
@@ -735,6 +760,13 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
     int evals = 0;
 
     while (st.phase != PH_DONE && evals < max_evals) {
+#ifdef FL_CHECKED
+        if (!state_in_bounds(d, st)) {
+            st.status = ST_CHECK;
+            st.phase = PH_DONE;
+            continue;
+        }
+#endif
         // ------------------------------------------------ phases without an RHS
         if (st.phase == PH_SEED) {
             // terminal seed λ̃(L) (interaction frame) into lam[0]
@@ -1140,6 +1172,13 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                     st.ck_stride *= 2;
                     slotc = st.nsteps / st.ck_stride;
                 }
+#ifdef FL_CHECKED
+                if (slotc < 0 || slotc >= d.ck_cap) {
+                    st.status = ST_CHECK;
+                    st.phase = PH_DONE;
+                    continue;
+                }
+#endif
                 const double* un = d.u[st.cur];
                 const CF* k1 = SolF::kp(d.kf, st.kperm, 0);
 #pragma unroll

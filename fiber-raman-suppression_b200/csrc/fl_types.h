@@ -39,7 +39,8 @@ enum : int {
     ST_NONFINITE = 2,
     ST_DT_UNDERFLOW = 3,
     ST_MAXITERS = 4,
-    ST_CAPACITY = 9
+    ST_CAPACITY = 9,
+    ST_CHECK = 14            // checked build: a state index left its buffer's bounds
 };
 
 // Per-slot pointers and parameters.  The forward solve and its recompute

@@ -12,12 +12,16 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libfiberlab_gpu.so")
+# FIBERLAB_GPU_LIB selects another in-tree build of the same C-ABI, e.g. the
+# bounds-checked libfiberlab_gpu_checked.so
+LIB_PATH = os.environ.get("FIBERLAB_GPU_LIB") or os.path.join(_HERE, "libfiberlab_gpu.so")
+CHECKED_LIB_PATH = os.path.join(_HERE, "libfiberlab_gpu_checked.so")
 
 FL_OK = 0
 STATUS = {0: "FL_OK", 1: "FL_EINVAL", 2: "FL_NONFINITE", 3: "FL_DT_UNDERFLOW", 4: "FL_MAXITERS",
           5: "FL_ENOMEM", 6: "FL_NONSYMMETRIC", 7: "FL_ENODEV", 8: "FL_ECUDA", 9: "FL_ECAPACITY",
-          10: "FL_EUNSUPPORTED", 11: "FL_OOM_ADMISSION", 12: "FL_EBUSY", 13: "FL_TIMEOUT"}
+          10: "FL_EUNSUPPORTED", 11: "FL_OOM_ADMISSION", 12: "FL_EBUSY", 13: "FL_TIMEOUT",
+          14: "FL_ECHECK"}
 PRECISION = {"fp32": 0, "fp64": 1}
 
 # every exported symbol of include/fiberlab_gpu.h (checked by the CPU tests)

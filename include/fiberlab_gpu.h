@@ -49,6 +49,9 @@ extern "C" {
 #define FL_OOM_ADMISSION 11  /* serving: request larger than the HBM budget */
 #define FL_EBUSY 12          /* serving: request not finished */
 #define FL_TIMEOUT 13        /* serving: wait limit reached */
+#define FL_ECHECK 14         /* checked build (libfiberlab_gpu_checked.so): a solver state
+                                index left its buffer's bounds; the slot stopped before
+                                the access */
 
 #define FL_PRECISION_FP32 0  /* FP32 bulk, FP64 phase/norm/reductions/state */
 #define FL_PRECISION_FP64 1  /* all arithmetic in FP64 */
