@@ -362,9 +362,9 @@ def multimode_measure(ctx, dev, B, steps, warmup):
     out = {}
     fp = P.multimode_problem(3, 96, 16384, 10.0, 2.0, 5e-9, 200e-15, seed=0,
                              raman_threshold_thz=-2.0)
-    # the multimode forward keeps checkpoints only: a 16-step recompute
-    # buffer per slot is enough for 32 checkpoints of these solves
-    ctx = Context(ctx.device, checkpoints=32, segment_steps=16)
+    # a dense-output buffer of 160 steps holds these solves (~120 forward
+    # steps) whole: the adjoint recomputes nothing (820 MB per candidate)
+    ctx = Context(ctx.device, checkpoints=32, segment_steps=160)
     gp = GPUProblem(ctx, fp)
     ph = np.random.default_rng(4).standard_normal((B, fp.M, fp.nt))
     d_u0 = torch.from_numpy(np.ascontiguousarray(fp.uw0).view(np.float64).copy()).to(dev)
@@ -394,7 +394,7 @@ def multimode_measure(ctx, dev, B, steps, warmup):
     tc_flops = 2 * M ** 4 * N * 6 * (fwd_att + rec)
     out["config4"] = {
         "workload": f"config 4: M=10 HG(m+n<=3), Nt=2^14 over 10 ps, L=2 m, 5 nJ, {B} per-mode "
-                    "phase candidates N(0,1), fwd+adjoint, checkpoints 32 x 64",
+                    "phase candidates N(0,1), fwd+adjoint, 160 dense-output steps",
         "solves_per_s": B * steps / (sum(ms) / 1e3), "ms_per_batch": float(np.mean(ms)),
         "steps_per_solve": {"forward": fwd_att / B, "adjoint": adj_att / B,
                             "recomputed": rec / B},

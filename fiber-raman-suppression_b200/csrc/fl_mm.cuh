@@ -417,13 +417,18 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     else dst = static_cast<C*>(mm_kp(d.kf, st.kperm, st.stage));
 #pragma unroll
     for (int s = 0; s < E; s++) dst[off + tid + TT * s] = v[s];
+    // dense interpolant of this mode's part of the step: c0 = ũ_n,
+    // c_p = Σ_i r_ip k_i (Tsit5's free 4th-order interpolant).  A replayed
+    // step keeps it for the steps of the current sub-segment; a forward
+    // attempt keeps it at the step's index while the solve fits the buffer
+    // (a rejected attempt is overwritten by its retry), so a solve that fits
+    // needs no recompute for its adjoint.
     const SubSeg sb = sub_segment(d, st);
-    if (st.stage == 6 && ph == PH_REC && sb.seg_lo + st.rec_pos >= sb.lo) {
-        // dense interpolant of the replayed step, this mode's part:
-        // c0 = ũ_n, c_p = Σ_i r_ip k_i (Tsit5's free 4th-order interpolant),
-        // kept for the steps of the current sub-segment only
+    const bool keep_rec = ph == PH_REC && sb.seg_lo + st.rec_pos >= sb.lo;
+    const bool keep_fwd = ph == PH_FWD && d.step_cap > 0 && st.nsteps < d.seg_cap;
+    if (st.stage == 6 && (keep_rec || keep_fwd)) {
         const size_t NM = (size_t)N * d.M,
-                     base = (size_t)(sb.seg_lo + st.rec_pos - sb.lo) * 5 * NM;
+                     base = (size_t)(keep_rec ? sb.seg_lo + st.rec_pos - sb.lo : st.nsteps) * 5 * NM;
         C* sg = static_cast<C*>(d.seg);
         const double* un = d.u[st.cur];
 #pragma unroll 1
@@ -1164,12 +1169,20 @@ struct MmCtl {
         }
         st.abstol_adj = scl == 0.0 ? d.abstol : d.abstol * scl;  // sensitivity_disp_mmf.jl:324-325
         st.nrec = 0;
-        st.dense = 0;
-        st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
-        st.sub = last_sub(d, st, st.seg);
         st.acur = 0;
         st.akperm = 0;
         st.a_naccept = st.a_nreject = st.a_nf = st.a_iters = 0;
+        // every step's interpolant is in the buffer when the forward fit it:
+        // the adjoint runs L -> 0 without recompute or stops
+        st.dense = st.nsteps <= d.seg_cap ? 1 : 0;
+        if (st.dense) {
+            st.seg = 0;
+            st.sub = 0;
+            st.phase = PH_ADJ_INIT;
+            return;
+        }
+        st.seg = (st.nsteps + st.ck_stride - 1) / st.ck_stride - 1;
+        st.sub = last_sub(d, st, st.seg);
         restore_checkpoint(st.seg);
         st.phase = PH_REC;
     }

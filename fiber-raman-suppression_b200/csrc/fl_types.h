@@ -183,7 +183,7 @@ struct MmState {
     long a_naccept, a_nreject, a_nf;
     long iters, a_iters;
     long nrec;              // forward steps recomputed for the adjoint
-    int dense;              // always 0: the multimode forward keeps checkpoints only
+    int dense;              // the forward kept every step's interpolant: no recompute
 };
 
 // ---------------------------------------------------------------------------

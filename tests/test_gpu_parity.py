@@ -316,9 +316,9 @@ def test_adjoint_beyond_checkpoint_capacity(gpu_ctx, caps):
     # segment is replayed once per sub-segment of segment_steps steps (no
     # FL_ECAPACITY); the gradient matches the oracle and the default layout
     K, seg = caps
-    fp = P.single_mode_problem(nt=256, time_window_ps=3.0, L=3.0, power_w=0.3,
-                               rep_rate_hz=80.5e6, raman_threshold_thz=-3.0)
-    phi = 0.3 * np.random.default_rng(31).standard_normal(fp.nt)
+    fp = P.single_mode_problem(nt=1024, time_window_ps=10.0, L=0.5, power_w=0.1,
+                               rep_rate_hz=80.5e6, raman_threshold_thz=-5.0)
+    phi = 0.5 * np.random.default_rng(31).standard_normal(fp.nt)
     J, g, st = GPUProblem(Context(0, checkpoints=K, segment_steps=seg), fp).phase_gradient_batch(
         phi[None, :])
     assert st[0]["status"] == 0 and st[0]["naccept"] > K * seg
