@@ -290,7 +290,9 @@ def serving_measure(ctx_cls, dev_index, n, window_s, plain_window_s, seed=3):
             stop.set()
         try:
             msg = q.get(timeout=max(0.05, min(left, 1.0)) if left > 0 else 120.0)
-        except Exception:
+        except Exception:                          # nothing finished meanwhile
+            if left > 0:
+                continue
             break                                  # a request outlived the grace period
         if msg[0] == "end":
             ended = True
