@@ -289,7 +289,7 @@ def serving_measure(ctx_cls, dev_index, n, window_s, plain_window_s, seed=3):
         if left <= 0 and not stop.is_set():
             stop.set()
         try:
-            msg = q.get(timeout=max(0.05, min(left, 1.0)) if left > 0 else 120.0)
+            msg = q.get(timeout=max(0.05, min(left, 1.0)) if left > 0 else 60.0)
         except Exception:                          # nothing finished meanwhile
             if left > 0:
                 continue
