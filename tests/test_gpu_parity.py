@@ -310,7 +310,7 @@ def test_status_codes_without_a_fault(gpu_ctx):
         assert e.value.status == 1
 
 
-@pytest.mark.parametrize("caps", [(2, 1), (4, 3), (8, 5)])
+@pytest.mark.parametrize("caps", [(2, 1), (4, 3), (4, 7)])
 def test_adjoint_beyond_checkpoint_capacity(gpu_ctx, caps):
     # more accepted steps than checkpoints x segment_steps: each checkpoint
     # segment is replayed once per sub-segment of segment_steps steps (no
