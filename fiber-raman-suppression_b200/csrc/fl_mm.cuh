@@ -1137,26 +1137,6 @@ struct MmCtl {
             double a[kMmMaxModes], r[kMmMaxModes];
             double cost;
             int pk = -1;
-            // FP32 mode: a band bin counts only above the FP32 round-off floor
-            // (its mode-summed energy above 2^-40 of the strongest bin's),
-            // as in the single-mode seed; FP64 mode keeps every bin
-            double gate = 0.0;
-            if (!d.fp64) {
-                double pk_e = 0.0;
-                for (int t = threadIdx.x; t < N; t += kMmCtl) {
-                    double e = 0.0;
-                    for (int m = 0; m < M; m++) e += energy(ld2(uf, (size_t)m * N + t));
-                    pk_e = fmax(pk_e, e);
-                }
-                gate = maxv(pk_e) * kBandGateFP32;
-            }
-            auto in_band = [&](int t) {
-                if (!d.mask[t]) return false;
-                if (gate == 0.0) return true;
-                double e = 0.0;
-                for (int m = 0; m < M; m++) e += energy(ld2(uf, (size_t)m * N + t));
-                return e > gate;
-            };
             if (obj == OBJ_FUNDAMENTAL || obj == OBJ_WORST_MODE) {
                 double tm[kMmMaxModes];
                 for (int m = 0; m < M; m++) {
@@ -1164,7 +1144,7 @@ struct MmCtl {
                     for (int t = threadIdx.x; t < N; t += kMmCtl) {
                         const double e = energy(ld2(uf, (size_t)m * N + t));
                         et += e;
-                        if (in_band(t)) eb += e;
+                        if (d.mask[t]) eb += e;
                     }
                     tm[m] = sum(et);
                     const double bm = sum(eb);
@@ -1196,7 +1176,7 @@ struct MmCtl {
                     double e = 0.0;
                     for (int m = 0; m < M; m++) e += energy(ld2(uf, (size_t)m * N + t));
                     et += e;
-                    if (d.mask[t] && e > gate) {
+                    if (d.mask[t]) {
                         eb += e;
                         emax = fmax(emax, e);
                     }
@@ -1210,7 +1190,7 @@ struct MmCtl {
                     for (int t = threadIdx.x; t < N; t += kMmCtl) {
                         double e = 0.0;
                         for (int m = 0; m < M; m++) e += energy(ld2(uf, (size_t)m * N + t));
-                        if (d.mask[t] && e > gate && e == band) key = fmax(key, (double)(N - t));
+                        if (d.mask[t] && e == band) key = fmax(key, (double)(N - t));
                     }
                     pk = N - (int)maxv(key);
                 }
@@ -1230,7 +1210,7 @@ struct MmCtl {
                 const int m = (int)(i / N), t = (int)(i % N);
                 const cx<double> x = ld2(uf, i);
                 const double sel = obj == OBJ_RAMAN_PEAK ? (t == pk ? 1.0 : 0.0)
-                                                         : (in_band(t) ? 1.0 : 0.0);
+                                                         : (d.mask[t] ? 1.0 : 0.0);
                 const double f = a[m] * (sel - r[m]) * sc;
                 st2(lam, i, mk(x.re * f, x.im * f));
             }

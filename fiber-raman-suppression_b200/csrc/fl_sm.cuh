@@ -61,11 +61,6 @@ static __device__ __constant__ double kT5r[7][4] = {
     {0.0, -27.896526289197286, 65.09189467479366, -34.87065786149661},
     {0.0, 1.5, -4.0, 2.5}};
 
-// FP32 mode: the band objectives count a bin only above this fraction of the
-// strongest bin's energy (2^-40: amplitude 1e-6 of the peak, 20x above the
-// FP32 transforms' round-off floor)
-constexpr double kBandGateFP32 = 9.094947017729282e-13;
-
 // PI controller defaults of OrdinaryDiffEq for a 5th-order method
 constexpr double kBeta1 = 7.0 / 50.0, kBeta2 = 2.0 / 25.0, kGamma = 0.9;
 constexpr double kQmin = 0.2, kQmax = 10.0, kQoldInit = 1e-4;
@@ -1012,26 +1007,13 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 // weight 1).  The peak objective (:288-302) puts the strongest
                 // in-band bin (lowest index among equals) in place of the band.
                 const bool peak = d.objective == OBJ_RAMAN_PEAK;
-                // In FP32 mode a band bin counts only above the round-off floor
-                // of the FP32 transforms (energy 2^-40 of the strongest bin,
-                // amplitude 1e-6; the floor itself sits near 5e-8): below it
-                // the field is noise, whose share of J is below 1e-9 (config
-                // 1: 3e-8 of J), and an adjoint seeded with it resolves that
-                // noise with 10^4..10^5 steps.  FP64 mode keeps every bin.
-                double gate = 0.0;
-                if constexpr (sizeof(RF) == 4) {
-                    double pk_e = 0.0;
-#pragma unroll
-                    for (int s = 0; s < E; s++) pk_e = fmax(pk_e, energy(ld2(uf, SolF::bin(s))));
-                    gate = block_max<T>(pk_e, red) * kBandGateFP32;
-                }
                 double et = 0.0, eb = 0.0, emax = -1.0;
 #pragma unroll
                 for (int s = 0; s < E; s++) {
                     const int b = SolF::bin(s);
                     const double e = energy(ld2(uf, b));
                     et += e;
-                    if (d.mask[b] && e > gate) {
+                    if (d.mask[b]) {
                         eb += e;
                         emax = fmax(emax, e);
                     }
@@ -1046,8 +1028,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
 #pragma unroll
                     for (int s = 0; s < E; s++) {
                         const int b = SolF::bin(s);
-                        const double e = energy(ld2(uf, b));
-                        if (d.mask[b] && e > gate && e == band) key = fmax(key, (double)(N - b));
+                        if (d.mask[b] && energy(ld2(uf, b)) == band) key = fmax(key, (double)(N - b));
                     }
                     pk = N - (int)block_max<T>(key, red);
                 }
@@ -1063,8 +1044,7 @@ __global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
                 for (int s = 0; s < E; s++) {
                     const int b = SolF::bin(s);
                     const cx<double> x = ld2(uf, b);
-                    const double sel =
-                        peak ? (b == pk ? 1.0 : 0.0) : (d.mask[b] && energy(x) > gate ? 1.0 : 0.0);
+                    const double sel = peak ? (b == pk ? 1.0 : 0.0) : (d.mask[b] ? 1.0 : 0.0);
                     const double f = (sel - cost) * sc;
                     st2(lam, b, mk(x.re * f, x.im * f));
                 }
