@@ -580,74 +580,11 @@ __device__ __forceinline__ void mm_imx(const MmDesc& d, int t) {
     }
 }
 
-// adjoint, second pass (thread per time point t, all modes j at once: the
-// fields λ_t, u_t and the M(M+1)/2 pair sequences S'_q, C_q of the point are
-// read once instead of once per output mode):
-//   η_j = Σ_q S'_q g_qj - (1-fR) Σ_q (u_k u_l) conj(g_qj) + 2i Σ_i C_ij u_i,
-//   g_qj = Σ_i λ_i G[i,j,q], G read from the table Ga[(j*NP + q)*MP + i]
-// (warp-uniform rows: every thread of a block reads the same entries)
-template <int M>
-__device__ __forceinline__ void mm_contract_adj_all(const MmDesc& d, int t) {
-    using PS = MmPairs<M>;
-    constexpr int NP = PS::NP, MP = PS::MP;
-    const int N = d.N;
-    const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
-    const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
-    const double* sq = static_cast<const double*>(d.sq);
-    const double* cq = static_cast<const double*>(d.cq);
-    cx<double>* eta = static_cast<cx<double>*>(d.eta);
-    const double ofr = d.one_m_fR;
-    cx<double> la[MP], u[M];
-#pragma unroll
-    for (int i = 0; i < M; i++) {
-        la[i] = lt[(size_t)i * N + t];
-        u[i] = ut[(size_t)i * N + t];
-    }
-#pragma unroll
-    for (int i = M; i < MP; i++) la[i] = mk(0.0, 0.0);
-    double er[M], ei[M];
-#pragma unroll
-    for (int j = 0; j < M; j++) er[j] = ei[j] = 0.0;
-    int k = 0, l = 0;
-#pragma unroll 1
-    for (int q = 0; q < NP; q++) {
-        const double s = sq[(size_t)q * N + t];
-        const cx<double> w = cmul(u[k], u[l]);
-#pragma unroll
-        for (int j = 0; j < M; j++) {
-            const double* Gq = d.Ga + ((size_t)j * NP + q) * MP;
-            double gr = 0.0, gi = 0.0;
-#pragma unroll
-            for (int i = 0; i < MP; i += 2) {
-                const double2 g = __ldg(reinterpret_cast<const double2*>(Gq + i));
-                gr += g.x * la[i].re + g.y * la[i + 1].re;
-                gi += g.x * la[i].im + g.y * la[i + 1].im;
-            }
-            // S' g - (1-fR) w conj(g)
-            er[j] += s * gr - ofr * (w.re * gr + w.im * gi);
-            ei[j] += s * gi - ofr * (w.im * gr - w.re * gi);
-        }
-        if (++l == M) {  // next pair (k <= l), row-major over k
-            ++k;
-            l = k;
-        }
-    }
-    // 2i Σ_i C_ij u_i, C symmetric stored per pair (min, max)
-#pragma unroll
-    for (int j = 0; j < M; j++) {
-#pragma unroll
-        for (int i = 0; i < M; i++) {
-            const int a = i < j ? i : j, b = i < j ? j : i;
-            const int p = a * M - a * (a - 1) / 2 + (b - a);
-            const double c = cq[(size_t)p * N + t];
-            er[j] -= 2.0 * c * u[i].im;
-            ei[j] += 2.0 * c * u[i].re;
-        }
-        eta[(size_t)j * N + t] = mk(er[j], ei[j]);
-    }
-}
-
-// adjoint, second pass, one output mode (thread per (t, j)): the same sums
+// adjoint, second pass (thread per (t, j)):
+//   η_j = Σ_q S'_q g_q - (1-fR) Σ_q (u_k u_l) conj(g_q) + 2i Σ_i C_ij u_i,
+//   g_q = Σ_i λ_i G[i,j,q], read from the table Ga[(j*NP + q)*MP + i]
+// (a thread per time point for all j read the point's fields once but ran
+// 15 % slower on a 10-mode launch list: fewer threads, more registers)
 template <int M>
 __device__ __forceinline__ void mm_contract_adj(const MmDesc& d, int t, int j) {
     using PS = MmPairs<M>;
@@ -716,13 +653,8 @@ __global__ void __launch_bounds__(kMmTB)
     if (which != 0 && (!adj || sizeof(R) != 8)) return;
     const int g = blockIdx.x * kMmTB + threadIdx.x;
     if (which == 2) {
-        if constexpr (M >= 4) {  // all modes per thread: the point's fields read once
-            if (g >= d.N) return;
-            mm_contract_adj_all<M>(d, g);
-        } else {
-            if (g >= d.N * M) return;
-            mm_contract_adj<M>(d, g % d.N, g / d.N);
-        }
+        if (g >= d.N * M) return;
+        mm_contract_adj<M>(d, g % d.N, g / d.N);
         return;
     }
     if (g >= d.N) return;

@@ -104,7 +104,7 @@ cudaError_t contract_m(const MmRound& a, int which) {
     if constexpr (sizeof(R) == 4 && M >= 6) {
         if (which == 0 && a.tensor_cores && a.N % kTcRows == 0) return contract_tc<M>(a);
     }
-    const int n = (which == 2 && M < 4) ? a.N * M : a.N;
+    const int n = which == 2 ? a.N * M : a.N;
     const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);
     mm_contract_kernel<R, M><<<grid, kMmTB, 0, a.stream>>>(static_cast<const MmDesc*>(a.desc),
                                                           a.state, a.active, which);
