@@ -182,6 +182,8 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
         const double* x = fw ? d.u[cur] : d.lam[cur];
         const double dt = st.cdt;
         if (st.stage < 6) {
+            // a checkpoint due at this step's start (set by the control kernel)
+            const int ckp = ph == PH_FWD && st.stage == 1 ? st.ck_pend : 0;
 #pragma unroll
             for (int s = 0; s < E; s++) {
                 const size_t b = off + tid + TT * s;
@@ -191,8 +193,10 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
                     const double a = kT5a[st.stage][j];
                     ar += a * (double)kj.re;
                     ai += a * (double)kj.im;
+                    if (ckp && j == 0) static_cast<C*>(d.ck_k1)[(size_t)(ckp - 1) * NM + b] = kj;
                 }
                 const cx<double> un = ld2(x, b);
+                if (ckp) st2(d.ck_u, (size_t)(ckp - 1) * NM + b, un);
                 v[s] = mk((R)(un.re + dt * ar), (R)(un.im + dt * ai));
             }
         } else {
@@ -773,6 +777,7 @@ struct MmCtl {
                 st.kperm = 0;
                 st.nsteps = 0;
                 st.ck_stride = 1;
+                st.ck_pend = 0;
                 st.naccept = st.nreject = st.iters = 0;
                 st.nf = 3;
                 if (d.ck_cap > 0) store_checkpoint(0, d.u0, d.kf[0]);
@@ -796,6 +801,7 @@ struct MmCtl {
         }
         if (ph == PH_FWD || ph == PH_REC) {
             if (st.stage < 6) {
+                if (st.stage == 1) st.ck_pend = 0;  // stored by this round's prologue
                 st.stage++;
                 return;
             }
@@ -894,8 +900,15 @@ struct MmCtl {
                     st.ck_stride *= 2;
                     slotc = st.nsteps / st.ck_stride;
                 }
-                __syncthreads();
-                store_checkpoint(slotc, d.u[st.cur], mm_kp(d.kf, st.kperm, 0));
+                if (znew == d.L) {
+                    __syncthreads();
+                    store_checkpoint(slotc, d.u[st.cur], mm_kp(d.kf, st.kperm, 0));
+                } else {
+                    // the next step's stage-1 prologue loads exactly u_n and
+                    // k1 in all of its mode groups: it stores the checkpoint
+                    // (one CTA copying 2-4 MB here was latency-bound)
+                    st.ck_pend = slotc + 1;
+                }
             }
             if (st.z == d.L) {
                 for (int si = st.save_idx; si < d.nsave; si++)

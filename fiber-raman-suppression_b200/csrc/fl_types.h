@@ -184,6 +184,7 @@ struct MmState {
     long iters, a_iters;
     long nrec;              // forward steps recomputed for the adjoint
     int dense;              // the forward kept every step's interpolant: no recompute
+    int ck_pend;            // checkpoint slot + 1 the next step's first prologue stores (0: none)
 };
 
 // ---------------------------------------------------------------------------
