@@ -643,17 +643,10 @@ __device__ __forceinline__ void mm_contract_adj(const MmDesc& d, int t, int j) {
 }
 
 // which = 0: forward contraction in R; 1: adjoint Im X; 2: adjoint assembly
-//
-// WHICH is a template parameter so each contraction is its own kernel with
-// its own register allocation: compiled together, the Im X path's 56-value
-// register array set every path's budget to 254 registers (two 128-thread
-// blocks per SM), the adjoint assembly's included.  The assembly is held to
-// 128 registers (four blocks per SM).
-template <typename R, int M, int WHICH>
-__global__ void __launch_bounds__(kMmTB, WHICH == 2 ? 4 : 1)
+template <typename R, int M>
+__global__ void __launch_bounds__(kMmTB)
     mm_contract_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
-                       const int* __restrict__ active) {
-    constexpr int which = WHICH;
+                       const int* __restrict__ active, int which) {
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
     if (d.M != M) return;
@@ -663,16 +656,14 @@ __global__ void __launch_bounds__(kMmTB, WHICH == 2 ? 4 : 1)
     if (which == 0 && adj) return;
     if (which != 0 && (!adj || sizeof(R) != 8)) return;
     const int g = blockIdx.x * kMmTB + threadIdx.x;
-    if constexpr (WHICH == 2) {
+    if (which == 2) {
         if (g >= d.N * M) return;
         mm_contract_adj<M>(d, g % d.N, g / d.N);
-    } else if constexpr (WHICH == 0) {
-        if (g >= d.N) return;
-        mm_contract_fwd<R, M>(d, g);
-    } else {
-        if (g >= d.N) return;
-        mm_imx<M>(d, g);
+        return;
     }
+    if (g >= d.N) return;
+    if (which == 0) mm_contract_fwd<R, M>(d, g);
+    else mm_imx<M>(d, g);
 }
 
 // ---------------------------------------------------------------------------

@@ -106,13 +106,8 @@ cudaError_t contract_m(const MmRound& a, int which) {
     }
     const int n = which == 2 ? a.N * M : a.N;
     const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);
-    const MmDesc* desc = static_cast<const MmDesc*>(a.desc);
-    if (which == 0)
-        mm_contract_kernel<R, M, 0><<<grid, kMmTB, 0, a.stream>>>(desc, a.state, a.active);
-    else if (which == 1)
-        mm_contract_kernel<R, M, 1><<<grid, kMmTB, 0, a.stream>>>(desc, a.state, a.active);
-    else
-        mm_contract_kernel<R, M, 2><<<grid, kMmTB, 0, a.stream>>>(desc, a.state, a.active);
+    mm_contract_kernel<R, M><<<grid, kMmTB, 0, a.stream>>>(static_cast<const MmDesc*>(a.desc),
+                                                          a.state, a.active, which);
     return cudaGetLastError();
 }
 
