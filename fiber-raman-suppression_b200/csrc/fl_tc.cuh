@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "fl_fft.cuh"
 #include "fl_types.h"
 
 namespace fl {
@@ -319,6 +320,320 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
                      "r"(128));
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint assembly of FP32-forward batches (M >= 6).  Per time point the
+// FP64 assembly (sensitivity_disp_mmf.jl:94-140)
+//   η_j = Σ_q S'_q g_qj - (1-fR) Σ_q w_q conj(g_qj) + 2i Σ_i C_ij u_i,
+//   g_qj = Σ_i λ_i G[i,j,q],   w_q = u_k u_l  (q = (k, l), k <= l)
+// regroups, G being real, into
+//   η_j = Σ_i [λ_i D'_ij - (1-fR) conj(λ_i) W_ij] + 2i Σ_i C_ij u_i,
+//   D'_ij = Σ_q G[i,j,q] S'_q,   W_ij = Σ_q G[i,j,q] w_q.
+// D' and W depend on the forward field alone, which the FP32 forward knows
+// to FP32 accuracy: they are three GEMMs of the forward contraction's shape
+// (A = S', Re w, Im w over a 128-point tile; B = G) on the tensor cores in
+// 3xTF32, while λ, C and the sums over i stay in FP64.  This takes the
+// assembly from about 14 300 FP64 FMAs per time point (10 modes) to 800.
+//
+// B rows hold (i, j) at i*16 + j, so row i of each accumulator is one
+// 16-column tensor-memory load; the three accumulators sit CS columns apart
+// in a 512-column allocation.  Two A buffers: S' and Re w are staged while
+// the MMAs of the other run; Im w reuses the first buffer once its MMAs have
+// completed.  Waits are bounded as in the forward contraction (a timeout
+// sets the tile's outputs to NaN) and tensor memory is freed on every path.
+template <int M>
+struct TcAdjShape {
+    static constexpr int NP = M * (M + 1) / 2;
+    static constexpr int KP = tc_kp(M);
+    static constexpr int NN = 16 * M;                   // MMA N: rows i*16 + j
+    static constexpr int CS = (NN + 31) & ~31;          // columns between accumulators
+    static constexpr int SBO = KP * 32;
+    static constexpr int A_BYTES = kTcRows * KP * 4;    // one of A_hi / A_lo
+    static constexpr int B_BYTES = NN * KP * 4;         // one of B_hi / B_lo
+    static constexpr int SMEM = 4 * A_BYTES + 2 * B_BYTES + 64 + 1024;
+    static constexpr uint32_t TMEM_COLS = 512;
+    // launched with at least 116 KB so that one CTA holds an SM and its
+    // 512 tensor-memory columns (no second allocation waits on the first)
+    static constexpr int SMEM_LAUNCH = SMEM > 116 * 1024 ? SMEM : 116 * 1024;
+    static_assert(NN <= 256, "MMA N");
+    static_assert(3 * CS <= (int)TMEM_COLS, "accumulator columns");
+    static_assert(SMEM <= 227 * 1024, "shared memory");
+};
+
+__host__ __device__ constexpr uint32_t tc_adj_bytes(int M) { return 2u * 16u * M * tc_kp(M) * 4u; }
+
+// bounded wait on an mbarrier phase (true: the phase completed)
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, long bound) {
+    uint32_t done = 0;
+    for (long it = 0; it < bound && !done; it++) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+    }
+    return done != 0;
+}
+
+// 3 x KP/8 MMAs (3xTF32) of one A tile against B into the accumulator at col
+template <int KP, int NN>
+__device__ __forceinline__ void tc_issue3(uint32_t tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
+                                          uint32_t b_lo) {
+    constexpr uint32_t idesc = tc_idesc(NN);
+    constexpr uint32_t sbo = KP * 32;
+#pragma unroll
+    for (int ks = 0; ks < KP / 8; ks++) {
+        const uint32_t koff = (uint32_t)ks * 256;
+        const uint64_t dah = tc_desc(a_hi + koff, 128, sbo);
+        const uint64_t dal = tc_desc(a_lo + koff, 128, sbo);
+        const uint64_t dbh = tc_desc(b_hi + koff, 128, sbo);
+        const uint64_t dbl = tc_desc(b_lo + koff, 128, sbo);
+        const uint32_t acc0 = ks > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
+    }
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, "
+        "%9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
+}
+
+// One A tile (this thread's row = time point) in the K-major layout, split
+// TF32 hi/lo: op 0 = S'_q, op 1 = Re w_q, op 2 = Im w_q; zeros for q >= NP.
+template <int M, int KP>
+__device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned char* Alo,
+                                            const double* __restrict__ sq, size_t N, int t,
+                                            const cx<float> (&uf)[M]) {
+    const int tid = threadIdx.x;
+    float h[4], l[4];
+    int q = 0;
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+#pragma unroll
+        for (int k2 = k; k2 < M; k2++) {
+            float x;
+            if (op == 0) {
+                x = (float)sq[(size_t)q * N + t];
+            } else {
+                const cx<float> w = cmul(uf[k], uf[k2]);
+                x = op == 1 ? w.re : w.im;
+            }
+            h[q & 3] = tf32_rn(x);
+            l[q & 3] = tf32_rn(x - h[q & 3]);
+            if ((q & 3) == 3) {
+                *reinterpret_cast<float4*>(Ahi + tc_off<KP>(tid, q - 3)) = make_float4(h[0], h[1], h[2], h[3]);
+                *reinterpret_cast<float4*>(Alo + tc_off<KP>(tid, q - 3)) = make_float4(l[0], l[1], l[2], l[3]);
+            }
+            q++;
+        }
+    }
+#pragma unroll
+    for (int r = M * (M + 1) / 2; r < KP; r++) {
+        h[r & 3] = 0.f;
+        l[r & 3] = 0.f;
+        if ((r & 3) == 3) {
+            *reinterpret_cast<float4*>(Ahi + tc_off<KP>(tid, r - 3)) = make_float4(h[0], h[1], h[2], h[3]);
+            *reinterpret_cast<float4*>(Alo + tc_off<KP>(tid, r - 3)) = make_float4(l[0], l[1], l[2], l[3]);
+        }
+    }
+}
+
+// The adjoint assembly of the 128-point tile `tile` of one slot.
+template <int M>
+__device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* smem) {
+    using TS = TcAdjShape<M>;
+    constexpr int NP = TS::NP, KP = TS::KP, NN = TS::NN, CS = TS::CS;
+    static_assert(KP % 4 == 0, "float4 groups");
+    const size_t N = (size_t)d.N;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int t = tile * kTcRows + tid;
+    unsigned char* base =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+    unsigned char* Xhi = base;
+    unsigned char* Xlo = Xhi + TS::A_BYTES;
+    unsigned char* Yhi = Xlo + TS::A_BYTES;
+    unsigned char* Ylo = Yhi + TS::A_BYTES;
+    unsigned char* Bhi = Ylo + TS::A_BYTES;
+    unsigned char* Blo = Bhi + TS::B_BYTES;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // X MMAs, Y MMAs, B image
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3);
+    uint32_t* bfail = tmem_slot + 1;
+    const uint32_t barX = smem_u32(bars), barY = smem_u32(bars + 1), barB = smem_u32(bars + 2);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(TS::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    constexpr uint32_t kBBytes = 2 * TS::B_BYTES, kBChunk = 16384;
+    static_assert(kBBytes % 16 == 0, "bulk copy size");
+    if (tid == 0) {
+        *bfail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barX));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barY));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barB));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
+                     "r"(kBBytes)
+                     : "memory");
+        const char* src = reinterpret_cast<const char*>(d.Gtca);
+        for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
+            const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                "[%3];" ::"r"(smem_u32(Bhi) + off),
+                "l"(src + off), "r"(n), "r"(barB)
+                : "memory");
+        }
+    }
+
+    const double* sq = static_cast<const double*>(d.sq);
+    const double* cq = static_cast<const double*>(d.cq);
+    const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
+    const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
+    cx<double>* eta = static_cast<cx<double>*>(d.eta);
+    cx<float> uf[M];
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        const cx<double> x = ut[(size_t)i * N + t];
+        uf[i] = mk((float)x.re, (float)x.im);
+    }
+
+    // ---- S' into X, then its MMAs (after a bounded wait for the B image)
+    tc_adj_fill<M, KP>(0, Xhi, Xlo, sq, N, t, uf);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const uint32_t bh = smem_u32(Bhi), bl = smem_u32(Blo);
+    if (tid == 0) {
+        if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
+        if (!*bfail) tc_issue3<KP, NN>(tmem, smem_u32(Xhi), smem_u32(Xlo), bh, bl);
+        tc_commit(barX);  // arrives once the MMAs above (if any) have completed
+    }
+    // ---- Re w into Y and its MMAs
+    tc_adj_fill<M, KP>(1, Yhi, Ylo, sq, N, t, uf);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0) {
+        if (!*bfail) tc_issue3<KP, NN>(tmem + CS, smem_u32(Yhi), smem_u32(Ylo), bh, bl);
+        tc_commit(barY);
+    }
+    // ---- Im w into X once the S' MMAs have read it
+    bool okX = tc_wait(barX, 0, 1L << 26);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (okX) tc_adj_fill<M, KP>(2, Xhi, Xlo, sq, N, t, uf);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    okX = __syncthreads_and(okX ? 1 : 0) != 0;  // block-uniform: a second X commit only if all saw the first
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (tid == 0 && okX) {
+        if (!*bfail) tc_issue3<KP, NN>(tmem + 2 * CS, smem_u32(Xhi), smem_u32(Xlo), bh, bl);
+        tc_commit(barX);
+    }
+    // ---- η_j = 2i Σ_i C_ij u_i + Σ_i [λ_i D'_ij - (1-fR) conj(λ_i) W_ij]; the
+    // FP64 loads and the C term run while the tensor cores finish
+    cx<double> la[M];
+#pragma unroll
+    for (int i = 0; i < M; i++) la[i] = lt[(size_t)i * N + t];
+    double er[M], ei[M];
+    {
+        cx<double> u[M];
+#pragma unroll
+        for (int i = 0; i < M; i++) {
+            u[i] = ut[(size_t)i * N + t];
+            er[i] = 0.0;
+            ei[i] = 0.0;
+        }
+        int p = 0;
+#pragma unroll
+        for (int a = 0; a < M; a++) {
+#pragma unroll
+            for (int b = a; b < M; b++) {
+                const double c2 = 2.0 * cq[(size_t)p * N + t];
+                er[b] -= c2 * u[a].im;
+                ei[b] += c2 * u[a].re;
+                if (a != b) {
+                    er[a] -= c2 * u[b].im;
+                    ei[a] += c2 * u[b].re;
+                }
+                p++;
+            }
+        }
+    }
+    const bool okY = tc_wait(barY, 0, 1L << 26);
+    const bool okX2 = okX && tc_wait(barX, 1, 1L << 26);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool ok = __syncthreads_and((okY && okX2) ? 1 : 0) != 0 && !*bfail;
+
+    if (ok) {
+        const double ofr = d.one_m_fR;
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int i = 0; i < M; i++) {
+            const cx<double> l = la[i];
+            float Dv[16], Wr[16], Wi[16];
+            tc_ld16(trow + (uint32_t)(i * 16), Dv);
+            tc_ld16(trow + (uint32_t)(CS + i * 16), Wr);
+            tc_ld16(trow + (uint32_t)(2 * CS + i * 16), Wi);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < M; j++) {
+                const double dv = Dv[j], wr = Wr[j], wi = Wi[j];
+                er[j] += l.re * dv - ofr * (l.re * wr + l.im * wi);
+                ei[j] += l.im * dv - ofr * (l.re * wi - l.im * wr);
+            }
+        }
+    }
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll
+    for (int j = 0; j < M; j++) eta[(size_t)j * N + t] = ok ? mk(er[j], ei[j]) : mk(nan, 0.0);
+
+    // ---- cleanup: a B copy that timed out, or MMAs whose completion a
+    // timed-out wait did not see, may still be in flight; wait for them
+    // (bounded) before shared and tensor memory are released
+    if (tid == 0) {
+        if (*bfail) tc_wait(barB, 0, 1L << 26);
+        if (!okX) {
+            tc_wait(barX, 0, 1L << 30);
+        } else if (!okX2) {
+            tc_wait(barX, 1, 1L << 30);
+        }
+        if (!okY) tc_wait(barY, 0, 1L << 30);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
+                     "r"(TS::TMEM_COLS));
 }
 
 }  // namespace fl

@@ -65,7 +65,11 @@ def test_mm_rhs_matches_oracle(gpu_ctx, M, nt, precision):
     z = 0.1234
     tol = 2e-6 if precision == "fp32" else FIELD_TOL_FP64
     assert rel(gp.rhs(z, u), O.rhs_forward(fp, z, u)) < tol
-    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < FIELD_TOL_FP64
+    # the adjoint runs in FP64; with an FP32 forward and M >= 6 its
+    # contractions of the forward field alone (G S', G u_k u_l) run on the
+    # tensor cores in 3xTF32, to the FP32 accuracy the forward field has
+    atol = 2e-6 if precision == "fp32" and M >= 6 else FIELD_TOL_FP64
+    assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < atol
 
 
 def test_mm_nonsymmetric_gamma_forward_only(gpu_ctx):
