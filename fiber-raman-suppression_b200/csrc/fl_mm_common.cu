@@ -98,7 +98,34 @@ __global__ void __launch_bounds__(kTcRows, 1)
     mm_contract_adj_tc<M>(d, blockIdx.x, tc_smem);
 }
 
+// The adjoint's Im X contraction of FP32-forward batches on the tensor
+// cores (M >= 6, Nt a multiple of 128): one 128-point tile per CTA.
+template <int M>
+__global__ void __launch_bounds__(kTcRows, 1)
+    mm_imx_tc_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
+                     const int* __restrict__ active) {
+    extern __shared__ __align__(16) unsigned char tc_smem[];
+    const int slot = active[blockIdx.y];
+    const MmDesc& d = descs[slot];
+    if (d.M != M || d.fp64) return;
+    const MmState st = states[slot];
+    if (!mm_takes<double>(d, st) || !mm_adjoint_phase(st.phase)) return;
+    mm_imx_tc<M>(d, blockIdx.x, tc_smem);
+}
+
 namespace {
+
+template <int M>
+cudaError_t imx_tc(const MmRound& a) {
+    const size_t smem = TcShape<M>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(mm_imx_tc_kernel<M>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(a.N / kTcRows, a.nactive);
+    mm_imx_tc_kernel<M><<<grid, kTcRows, smem, a.stream>>>(static_cast<const MmDesc*>(a.desc),
+                                                          a.state, a.active);
+    return cudaGetLastError();
+}
 
 template <int M>
 cudaError_t contract_adj_tc(const MmRound& a) {
@@ -132,11 +159,13 @@ cudaError_t contract_m(const MmRound& a, int which) {
     if constexpr (sizeof(R) == 4 && M >= 6) {
         if (which == 0 && a.tensor_cores && a.N % kTcRows == 0) return contract_tc<M>(a);
     }
-    // adjoint assembly of an FP32-forward batch with M >= 6 modes: the
-    // forward-field contractions on the tensor cores, the rest in FP64
+    // adjoint of an FP32-forward batch with M >= 6 modes: the assembly's
+    // forward-field contractions and the Im X contraction on the tensor
+    // cores (3xTF32), the rest in FP64
     if constexpr (sizeof(R) == 8 && M >= 6) {
         if (which == 2 && !a.fp64 && a.tensor_cores && a.N % kTcRows == 0)
             return contract_adj_tc<M>(a);
+        if (which == 1 && !a.fp64 && a.tensor_cores && a.N % kTcRows == 0) return imx_tc<M>(a);
     }
     const int n = which == 2 ? a.N * M : a.N;
     const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);

@@ -426,11 +426,9 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 // One A tile (this thread's row = time point) in the K-major layout, split
-// TF32 hi/lo: op 0 = S'_q, op 1 = Re w_q, op 2 = Im w_q; zeros for q >= NP.
-template <int M, int KP>
-__device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned char* Alo,
-                                            const double* __restrict__ sq, size_t N, int t,
-                                            const cx<float> (&uf)[M]) {
+// TF32 hi/lo: column q = pair (k, l) holds f(q, k, l); zeros for q >= NP.
+template <int M, int KP, class F>
+__device__ __forceinline__ void tc_fill_pairs(unsigned char* Ahi, unsigned char* Alo, F&& f) {
     const int tid = threadIdx.x;
     float h[4], l[4];
     int q = 0;
@@ -438,13 +436,7 @@ __device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned
     for (int k = 0; k < M; k++) {
 #pragma unroll
         for (int k2 = k; k2 < M; k2++) {
-            float x;
-            if (op == 0) {
-                x = (float)sq[(size_t)q * N + t];
-            } else {
-                const cx<float> w = cmul(uf[k], uf[k2]);
-                x = op == 1 ? w.re : w.im;
-            }
+            const float x = f(q, k, k2);
             h[q & 3] = tf32_rn(x);
             l[q & 3] = tf32_rn(x - h[q & 3]);
             if ((q & 3) == 3) {
@@ -463,6 +455,18 @@ __device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned
             *reinterpret_cast<float4*>(Alo + tc_off<KP>(tid, r - 3)) = make_float4(l[0], l[1], l[2], l[3]);
         }
     }
+}
+
+// the adjoint assembly's A tiles: op 0 = S'_q, op 1 = Re w_q, op 2 = Im w_q
+template <int M, int KP>
+__device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned char* Alo,
+                                            const double* __restrict__ sq, size_t N, int t,
+                                            const cx<float> (&uf)[M]) {
+    tc_fill_pairs<M, KP>(Ahi, Alo, [&](int q, int k, int l) -> float {
+        if (op == 0) return (float)sq[(size_t)q * N + t];
+        const cx<float> w = cmul(uf[k], uf[l]);
+        return op == 1 ? w.re : w.im;
+    });
 }
 
 // The adjoint assembly of the 128-point tile `tile` of one slot.
@@ -634,6 +638,115 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
                      "r"(TS::TMEM_COLS));
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint first pass of FP32-forward batches (M >= 6) on the tensor cores:
+//   Im X_p = Σ_q G[i,j,q] Y_q  for the pairs p = (i <= j),
+//   Y_q = (Im(λ_k u_l*) + Im(λ_l u_k*))/2 (k < l), Im(λ_k u_k*) (k = l),
+// the forward contraction's GEMM with A = Y (formed in FP64, split 3xTF32)
+// and the forward B image (rows i*M + j); the pairs i <= j of each
+// thread's accumulator row go to C's input table in FP64.  Waits are
+// bounded (a timeout writes NaN) and tensor memory is freed on every path.
+template <int M>
+__device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
+    using TS = TcShape<M>;
+    constexpr int KP = TS::KP, NN = TS::NN, NP = TS::NP;
+    const size_t N = (size_t)d.N;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int t = tile * kTcRows + tid;
+    unsigned char* base =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+    unsigned char* Ahi = base;
+    unsigned char* Alo = Ahi + TS::A_BYTES;
+    unsigned char* Bhi = Alo + TS::A_BYTES;
+    unsigned char* Blo = Bhi + TS::B_BYTES;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // MMAs, B image
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    uint32_t* bfail = tmem_slot + 1;
+    const uint32_t barM = smem_u32(bars), barB = smem_u32(bars + 1);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(128));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    constexpr uint32_t kBBytes = 2 * TS::B_BYTES, kBChunk = 16384;
+    static_assert(kBBytes % 16 == 0, "bulk copy size");
+    if (tid == 0) {
+        *bfail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barM));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barB));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
+                     "r"(kBBytes)
+                     : "memory");
+        const char* src = reinterpret_cast<const char*>(d.Gtc);
+        for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
+            const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                "[%3];" ::"r"(smem_u32(Bhi) + off),
+                "l"(src + off), "r"(n), "r"(barB)
+                : "memory");
+        }
+    }
+    const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
+    const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
+    double* cq = static_cast<double*>(d.cq);
+    cx<double> la[M], u[M];
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        la[i] = lt[(size_t)i * N + t];
+        u[i] = ut[(size_t)i * N + t];
+    }
+    tc_fill_pairs<M, KP>(Ahi, Alo, [&](int, int k, int l) -> float {
+        const double a = la[k].im * u[l].re - la[k].re * u[l].im;  // Im(λ_k u_l*)
+        if (k == l) return (float)a;
+        const double b = la[l].im * u[k].re - la[l].re * u[k].im;
+        return (float)(0.5 * (a + b));
+    });
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    if (tid == 0) {
+        if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
+        if (!*bfail) tc_issue3<KP, NN>(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo));
+        tc_commit(barM);
+    }
+    const bool done = tc_wait(barM, 0, 1L << 26);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool ok = __syncthreads_and(done ? 1 : 0) != 0 && !*bfail;
+    if (ok) {
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c = 0; c < NN; c += 16) {
+            float v[16];
+            tc_ld16(trow + (uint32_t)c, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const int col = c + e, i = col / M, j = col % M;
+                if (col < M * M && i <= j)
+                    cq[(size_t)(i * M - i * (i - 1) / 2 + (j - i)) * N + t] = (double)v[e];
+            }
+        }
+    } else {
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+#pragma unroll 1
+        for (int p = 0; p < NP; p++) cq[(size_t)p * N + t] = nan;
+    }
+    if (tid == 0) {
+        if (*bfail) tc_wait(barB, 0, 1L << 26);
+        if (!done) tc_wait(barM, 0, 1L << 30);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
+                     "r"(128));
 }
 
 }  // namespace fl
