@@ -561,6 +561,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         d.NP = w->np;
         d.N = pr->nt;
         d.fp64 = pr->precision == FL_PRECISION_FP64;
+        d.adj_mixed = mm_adj_mixed(d.M, d.N, d.fp64);
         d.one_m_fR = pr->one_m_fR;
         d.L = pr->L;
         d.reltol = pr->reltol;

@@ -145,104 +145,110 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     const int m = blockIdx.x / CL;
     if (m >= d.M) return;
     const MmState st = states[slot];
-    if (!mm_takes<R>(d, st)) return;
+    // a mixed-precision adjoint (mm_adj_mixed) transforms λ in the FP64
+    // kernel and the forward field in the FP32 one
+    const bool fwd_field = sizeof(R) == 4 && d.adj_mixed && mm_rhs_phase(st.phase) &&
+                           mm_adjoint_phase(st.phase);
+    if (!mm_takes<R>(d, st) && !fwd_field) return;
     G grp;
     grp.init(d, smraw);
     const int tid = grp.g;  // index in the transform group
     const size_t NM = (size_t)N * d.M, off = (size_t)m * N;
     const int ph = st.phase;
     const bool adj = mm_adjoint_phase(ph);
+    const double* Dt = d.Dturns + off;
     C v[E];
 
-    // ---- stage input (FP64 accumulation, as the single-mode stepper)
-    if (ph == PH_EVAL_FWD || ph == PH_EVAL_ADJ) {
+    if (!fwd_field) {
+        // ---- stage input (FP64 accumulation, as the single-mode stepper)
+        if (ph == PH_EVAL_FWD || ph == PH_EVAL_ADJ) {
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.u0, off + tid + TT * s));
-    } else if (ph == PH_FWD_INIT || ph == PH_ADJ_INIT) {
-        const bool fw = ph == PH_FWD_INIT;
-        const double* x0 = fw ? d.u0 : d.lam[0];
-        const C* k1 = static_cast<const C*>(fw ? d.kf[0] : d.ka[0]);
-        const double sg = fw ? st.cdt : -st.cdt;
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const size_t b = off + tid + TT * s;
-            const cx<double> x = ld2(x0, b);
-            if (st.stage == 0) {
-                v[s] = down<R>(x);
-            } else {
-                const C f0 = k1[b];
-                v[s] = mk((R)(x.re + sg * (double)f0.re), (R)(x.im + sg * (double)f0.im));
-            }
-        }
-    } else {
-        const bool fw = !adj;
-        void* const* K = fw ? d.kf : d.ka;
-        const int perm = fw ? st.kperm : st.akperm;
-        const int cur = fw ? st.cur : st.acur;
-        const double* x = fw ? d.u[cur] : d.lam[cur];
-        const double dt = st.cdt;
-        if (st.stage < 6) {
-            // a checkpoint due at this step's start (set by the control kernel)
-            const int ckp = ph == PH_FWD && st.stage == 1 ? st.ck_pend : 0;
+            for (int s = 0; s < E; s++) v[s] = down<R>(ld2(d.u0, off + tid + TT * s));
+        } else if (ph == PH_FWD_INIT || ph == PH_ADJ_INIT) {
+            const bool fw = ph == PH_FWD_INIT;
+            const double* x0 = fw ? d.u0 : d.lam[0];
+            const C* k1 = static_cast<const C*>(fw ? d.kf[0] : d.ka[0]);
+            const double sg = fw ? st.cdt : -st.cdt;
 #pragma unroll
             for (int s = 0; s < E; s++) {
                 const size_t b = off + tid + TT * s;
-                double ar = 0.0, ai = 0.0;
-                for (int j = 0; j < st.stage; j++) {
-                    const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
-                    const double a = kT5a[st.stage][j];
-                    ar += a * (double)kj.re;
-                    ai += a * (double)kj.im;
-                    if (ckp && j == 0) static_cast<C*>(d.ck_k1)[(size_t)(ckp - 1) * NM + b] = kj;
+                const cx<double> x = ld2(x0, b);
+                if (st.stage == 0) {
+                    v[s] = down<R>(x);
+                } else {
+                    const C f0 = k1[b];
+                    v[s] = mk((R)(x.re + sg * (double)f0.re), (R)(x.im + sg * (double)f0.im));
                 }
-                const cx<double> un = ld2(x, b);
-                if (ckp) st2(d.ck_u, (size_t)(ckp - 1) * NM + b, un);
-                v[s] = mk((R)(un.re + dt * ar), (R)(un.im + dt * ai));
             }
         } else {
-            double* xnew = fw ? d.u[cur ^ 1] : d.lam[cur ^ 1];
-            const bool want_err = ph != PH_REC;
-            const double at = fw ? d.abstol : st.abstol_adj, rt = d.reltol;
+            const bool fw = !adj;
+            void* const* K = fw ? d.kf : d.ka;
+            const int perm = fw ? st.kperm : st.akperm;
+            const int cur = fw ? st.cur : st.acur;
+            const double* x = fw ? d.u[cur] : d.lam[cur];
+            const double dt = st.cdt;
+            if (st.stage < 6) {
+                // a checkpoint due at this step's start (set by the control kernel)
+                const int ckp = ph == PH_FWD && st.stage == 1 ? st.ck_pend : 0;
 #pragma unroll
-            for (int s = 0; s < E; s++) {
-                const size_t b = off + tid + TT * s;
-                double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
-                for (int j = 0; j < 6; j++) {
-                    const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
-                    const double a = kT5a[6][j], bt = kT5bt[j];
-                    ar += a * (double)kj.re;
-                    ai += a * (double)kj.im;
-                    er += bt * (double)kj.re;
-                    ei += bt * (double)kj.im;
+                for (int s = 0; s < E; s++) {
+                    const size_t b = off + tid + TT * s;
+                    double ar = 0.0, ai = 0.0;
+                    for (int j = 0; j < st.stage; j++) {
+                        const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
+                        const double a = kT5a[st.stage][j];
+                        ar += a * (double)kj.re;
+                        ai += a * (double)kj.im;
+                        if (ckp && j == 0) static_cast<C*>(d.ck_k1)[(size_t)(ckp - 1) * NM + b] = kj;
+                    }
+                    const cx<double> un = ld2(x, b);
+                    if (ckp) st2(d.ck_u, (size_t)(ckp - 1) * NM + b, un);
+                    v[s] = mk((R)(un.re + dt * ar), (R)(un.im + dt * ai));
                 }
-                const cx<double> un = ld2(x, b);
-                const cx<double> u1 = mk(un.re + dt * ar, un.im + dt * ai);
-                st2(xnew, b, u1);
-                if (want_err) {
-                    st2(d.esv, b, mk(dt * er, dt * ei));
-                    const double m0 = sqrt(un.re * un.re + un.im * un.im);
-                    const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
-                    d.skv[b] = at + fmax(m0, m1) * rt;
+            } else {
+                double* xnew = fw ? d.u[cur ^ 1] : d.lam[cur ^ 1];
+                const bool want_err = ph != PH_REC;
+                const double at = fw ? d.abstol : st.abstol_adj, rt = d.reltol;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const size_t b = off + tid + TT * s;
+                    double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
+                    for (int j = 0; j < 6; j++) {
+                        const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
+                        const double a = kT5a[6][j], bt = kT5bt[j];
+                        ar += a * (double)kj.re;
+                        ai += a * (double)kj.im;
+                        er += bt * (double)kj.re;
+                        ei += bt * (double)kj.im;
+                    }
+                    const cx<double> un = ld2(x, b);
+                    const cx<double> u1 = mk(un.re + dt * ar, un.im + dt * ai);
+                    st2(xnew, b, u1);
+                    if (want_err) {
+                        st2(d.esv, b, mk(dt * er, dt * ei));
+                        const double m0 = sqrt(un.re * un.re + un.im * un.im);
+                        const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
+                        d.skv[b] = at + fmax(m0, m1) * rt;
+                    }
+                    v[s] = down<R>(u1);
                 }
-                v[s] = down<R>(u1);
             }
         }
-    }
 
-    // ---- to time: forward u_t = F(e^{iDz} ũ); adjoint λ_t = F(e^{iDz} τ λ̃)
-    const double* Dt = d.Dturns + off;
-    const R* ss = static_cast<const R*>(d.ss[P]);
-    C* out = static_cast<C*>(adj ? d.lt : d.ut);
+        // ---- to time: forward u_t = F(e^{iDz} ũ); adjoint λ_t = F(e^{iDz} τ λ̃)
+        const R* ss = static_cast<const R*>(d.ss[P]);
+        C* out = static_cast<C*>(adj ? d.lt : d.ut);
 #pragma unroll
-    for (int s = 0; s < E; s++) {
-        const int t = tid + TT * s;
-        v[s] = cmul(v[s], phasor<R>(Dt[t], st.ez));
-        if (adj) v[s] = scale(v[s], ss[t]);
+        for (int s = 0; s < E; s++) {
+            const int t = tid + TT * s;
+            v[s] = cmul(v[s], phasor<R>(Dt[t], st.ez));
+            if (adj) v[s] = scale(v[s], ss[t]);
+        }
+        grp.fft(v);
+#pragma unroll
+        for (int s = 0; s < E; s++) out[off + tid + TT * s] = v[s];
+        if (!adj || d.adj_mixed) return;  // (mixed: the FP32 kernel takes the forward field)
     }
-    grp.fft(v);
-#pragma unroll
-    for (int s = 0; s < E; s++) out[off + tid + TT * s] = v[s];
-    if (!adj) return;
 
     // ---- adjoint: the forward field at ezload, F(e^{iDz} ũ(z))
     if (ph == PH_EVAL_ADJ) {
@@ -304,12 +310,16 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
     const MmState st = states[slot];
-    if (!mm_takes<R>(d, st)) return;
-    const bool adj = mm_adjoint_phase(st.phase);
+    const bool adj = mm_rhs_phase(st.phase) && mm_adjoint_phase(st.phase);
+    // a mixed-precision adjoint (mm_adj_mixed) forms the products P of the
+    // forward field in the FP32 kernel and the Im X correlations in FP64
+    const bool mixed = adj && d.adj_mixed;
+    if (!mm_takes<R>(d, st) && !(mixed && sizeof(R) == 4)) return;
     const int M = d.M, NP = d.NP, ntp = (NP + 1) / 2;
     const int unit = blockIdx.x / CL;
     const bool ytask = unit >= ntp;  // correlation of Im X (adjoint only)
     if (ytask && !adj) return;
+    if (mixed && ytask != (sizeof(R) == 8)) return;
     const int q0 = 2 * (ytask ? unit - ntp : unit);
     if (q0 >= NP) return;
     const int q1 = q0 + 1;

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
     extern __shared__ __align__(16) unsigned char tc_smem[];
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
-    if (d.M != M || d.fp64) return;
+    if (d.M != M || !d.adj_mixed) return;
     const MmState st = states[slot];
     if (!mm_takes<double>(d, st) || !mm_adjoint_phase(st.phase)) return;
     mm_contract_adj_tc<M>(d, blockIdx.x, tc_smem);
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
     extern __shared__ __align__(16) unsigned char tc_smem[];
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
-    if (d.M != M || d.fp64) return;
+    if (d.M != M || !d.adj_mixed) return;
     const MmState st = states[slot];
     if (!mm_takes<double>(d, st) || !mm_adjoint_phase(st.phase)) return;
     mm_imx_tc<M>(d, blockIdx.x, tc_smem);
@@ -159,13 +159,11 @@ cudaError_t contract_m(const MmRound& a, int which) {
     if constexpr (sizeof(R) == 4 && M >= 6) {
         if (which == 0 && a.tensor_cores && a.N % kTcRows == 0) return contract_tc<M>(a);
     }
-    // adjoint of an FP32-forward batch with M >= 6 modes: the assembly's
-    // forward-field contractions and the Im X contraction on the tensor
-    // cores (3xTF32), the rest in FP64
+    // mixed-precision adjoint (mm_adj_mixed): the assembly's forward-field
+    // contractions and the Im X contraction on the tensor cores (3xTF32)
     if constexpr (sizeof(R) == 8 && M >= 6) {
-        if (which == 2 && !a.fp64 && a.tensor_cores && a.N % kTcRows == 0)
-            return contract_adj_tc<M>(a);
-        if (which == 1 && !a.fp64 && a.tensor_cores && a.N % kTcRows == 0) return imx_tc<M>(a);
+        if (which == 2 && mm_adj_mixed(M, a.N, a.fp64)) return contract_adj_tc<M>(a);
+        if (which == 1 && mm_adj_mixed(M, a.N, a.fp64)) return imx_tc<M>(a);
     }
     const int n = which == 2 ? a.N * M : a.N;
     const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);

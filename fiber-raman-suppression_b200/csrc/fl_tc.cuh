@@ -460,10 +460,10 @@ __device__ __forceinline__ void tc_fill_pairs(unsigned char* Ahi, unsigned char*
 // the adjoint assembly's A tiles: op 0 = S'_q, op 1 = Re w_q, op 2 = Im w_q
 template <int M, int KP>
 __device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned char* Alo,
-                                            const double* __restrict__ sq, size_t N, int t,
+                                            const float* __restrict__ sq, size_t N, int t,
                                             const cx<float> (&uf)[M]) {
     tc_fill_pairs<M, KP>(Ahi, Alo, [&](int q, int k, int l) -> float {
-        if (op == 0) return (float)sq[(size_t)q * N + t];
+        if (op == 0) return sq[(size_t)q * N + t];
         const cx<float> w = cmul(uf[k], uf[l]);
         return op == 1 ? w.re : w.im;
     });
@@ -519,17 +519,15 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
         }
     }
 
-    const double* sq = static_cast<const double*>(d.sq);
+    // the mixed adjoint's FP32 forward field and S' (the FP32 kernels' output)
+    const float* sq = static_cast<const float*>(d.sq);
     const double* cq = static_cast<const double*>(d.cq);
-    const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
+    const cx<float>* ut = static_cast<const cx<float>*>(d.ut);
     const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
     cx<double>* eta = static_cast<cx<double>*>(d.eta);
     cx<float> uf[M];
 #pragma unroll
-    for (int i = 0; i < M; i++) {
-        const cx<double> x = ut[(size_t)i * N + t];
-        uf[i] = mk((float)x.re, (float)x.im);
-    }
+    for (int i = 0; i < M; i++) uf[i] = ut[(size_t)i * N + t];
 
     // ---- S' into X, then its MMAs (after a bounded wait for the B image)
     tc_adj_fill<M, KP>(0, Xhi, Xlo, sq, N, t, uf);
@@ -573,7 +571,7 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
         cx<double> u[M];
 #pragma unroll
         for (int i = 0; i < M; i++) {
-            u[i] = ut[(size_t)i * N + t];
+            u[i] = mk((double)uf[i].re, (double)uf[i].im);
             er[i] = 0.0;
             ei[i] = 0.0;
         }
@@ -693,13 +691,14 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
         }
     }
     const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
-    const cx<double>* ut = static_cast<const cx<double>*>(d.ut);
+    const cx<float>* ut = static_cast<const cx<float>*>(d.ut);  // the mixed adjoint's FP32 field
     double* cq = static_cast<double*>(d.cq);
     cx<double> la[M], u[M];
 #pragma unroll
     for (int i = 0; i < M; i++) {
         la[i] = lt[(size_t)i * N + t];
-        u[i] = ut[(size_t)i * N + t];
+        const cx<float> x = ut[(size_t)i * N + t];
+        u[i] = mk((double)x.re, (double)x.im);
     }
     tc_fill_pairs<M, KP>(Ahi, Alo, [&](int, int k, int l) -> float {
         const double a = la[k].im * u[l].re - la[k].re * u[l].im;  // Im(λ_k u_l*)

@@ -112,6 +112,13 @@ struct SlotState {
 // (M(M+1)/2) padded to 4 and the mode axis padded to 2 (vector loads).
 __host__ __device__ constexpr int mm_gp(int M) { return (M * (M + 1) / 2 + 3) & ~3; }
 __host__ __device__ constexpr int mm_mp(int M) { return (M + 1) & ~1; }
+// The adjoint of an FP32-forward batch with M >= 6 modes on whole 128-point
+// tiles runs mixed: λ and everything linear in it in FP64, while the forward
+// field's transform and pair products (known to FP32 accuracy) run in FP32
+// and the contractions on the tensor cores (3xTF32).
+__host__ __device__ constexpr bool mm_adj_mixed(int M, int N, int fp64) {
+    return !fp64 && M >= 6 && N % 128 == 0;
+}
 
 // ---------------------------------------------------------------------------
 // Multimode (M > 1) slots.  One right-hand-side evaluation runs as a chain of
@@ -130,6 +137,7 @@ struct MmDesc {
     const float* Gtc;       // M >= 6: the tensor-core B operand (G split hi/lo, shared-memory image)
     const float* Gtca;      // M >= 6: the adjoint's B operand (rows (i, j) at i*16 + j, split hi/lo)
     int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
+    int adj_mixed;          // mm_adj_mixed(M, N, fp64): mixed-precision adjoint
     int nparts;             // error partial sums per evaluation (M x CTAs per transform)
     double one_m_fR;
     double L, reltol, abstol;

@@ -65,9 +65,10 @@ def test_mm_rhs_matches_oracle(gpu_ctx, M, nt, precision):
     z = 0.1234
     tol = 2e-6 if precision == "fp32" else FIELD_TOL_FP64
     assert rel(gp.rhs(z, u), O.rhs_forward(fp, z, u)) < tol
-    # the adjoint runs in FP64; with an FP32 forward and M >= 6 its
-    # contractions of the forward field alone (G S', G u_k u_l) run on the
-    # tensor cores in 3xTF32, to the FP32 accuracy the forward field has
+    # with an FP32 forward and M >= 6 the adjoint runs mixed: λ and its
+    # transforms in FP64, the forward field's transform and pair products in
+    # FP32 (the accuracy that field has) and the per-point contractions on
+    # the tensor cores in 3xTF32
     atol = 2e-6 if precision == "fp32" and M >= 6 else FIELD_TOL_FP64
     assert rel(gp.rhs(z, lam, u), O.rhs_adjoint(fp, z, lam, u)) < atol
 
