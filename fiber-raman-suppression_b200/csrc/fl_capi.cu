@@ -161,7 +161,7 @@ struct fl_problem {
     void* d_G[2] = {nullptr, nullptr};     // multimode contraction matrix [0] float, [1] double
     double* d_Ga = nullptr;                // its adjoint layout
     float* d_Gtc = nullptr;                // its tensor-core operand image (M >= 6)
-    float* d_Gtca = nullptr;               // the adjoint assembly's image (M >= 6)
+    float* d_Gtcs = nullptr;               // its symmetric image (pairs i <= j; M >= 6)
     // device staging of the host-buffer batch calls (grow-only, reused)
     char* d_stage = nullptr;
     size_t stage_bytes = 0;
@@ -555,7 +555,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         }
         d.Ga = pr->d_Ga;
         d.Gtc = pr->d_Gtc;
-        d.Gtca = pr->d_Gtca;
+        d.Gtcs = pr->d_Gtcs;
         d.M = pr->m;
         d.nparts = nparts;
         d.NP = w->np;
@@ -808,14 +808,15 @@ int mm_upload_G(fl_problem* pr, const double* gamma) {
             }
         CU(cudaMalloc(&pr->d_Gtc, img.size()));
         CU(cudaMemcpy(pr->d_Gtc, img.data(), img.size(), cudaMemcpyHostToDevice));
-        // B operand of the adjoint assembly: rows (i, j) at i*16 + j (zeros
-        // for j >= M), the same pairs, split and layout
-        const size_t abytes = (size_t)16 * M * KP * 4;
+        // the symmetric B operand of the adjoint contractions: row p holds
+        // G[i][j][.] = G[j][i][.] for the pairs p = (i <= j) (rows padded to
+        // 16 with zeros), the same pairs along K, split and layout
+        const int NS = (NP + 15) & ~15;
+        const size_t abytes = (size_t)NS * KP * 4;
         std::vector<unsigned char> aimg(2 * abytes, 0);
-        for (int i = 0; i < M; i++)
-            for (int j = 0; j < M; j++)
+        for (int i = 0, r = 0; i < M; i++)
+            for (int j = i; j < M; j++, r++)
                 for (int k = 0; k < NP; k++) {
-                    const int r = i * 16 + j;
                     const float g = Gf[((size_t)i * M + j) * GP + k];
                     const float hi = tf32(g), lo = tf32(g - hi);
                     const uint32_t off =
@@ -823,8 +824,8 @@ int mm_upload_G(fl_problem* pr, const double* gamma) {
                     memcpy(&aimg[off], &hi, 4);
                     memcpy(&aimg[abytes + off], &lo, 4);
                 }
-        CU(cudaMalloc(&pr->d_Gtca, aimg.size()));
-        CU(cudaMemcpy(pr->d_Gtca, aimg.data(), aimg.size(), cudaMemcpyHostToDevice));
+        CU(cudaMalloc(&pr->d_Gtcs, aimg.size()));
+        CU(cudaMemcpy(pr->d_Gtcs, aimg.data(), aimg.size(), cudaMemcpyHostToDevice));
     }
     return FL_OK;
 }
@@ -1157,7 +1158,7 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
         }
         d.Ga = pr->d_Ga;
         d.Gtc = pr->d_Gtc;
-        d.Gtca = pr->d_Gtca;
+        d.Gtcs = pr->d_Gtcs;
         d.one_m_fR = pr->one_m_fR;
         d.L = r->L;
         d.reltol = pr->reltol;
@@ -1625,7 +1626,7 @@ int fl_problem_destroy(fl_problem* pr) {
     cudaFree(pr->d_G[1]);
     cudaFree(pr->d_Ga);
     cudaFree(pr->d_Gtc);
-    cudaFree(pr->d_Gtca);
+    cudaFree(pr->d_Gtcs);
     cudaFree(pr->d_Dturns);
     for (int q = 0; q < 2; q++) {
         cudaFree(pr->d_Heff[q]);

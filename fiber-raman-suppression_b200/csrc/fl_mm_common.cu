@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kTcRows)
 // contractions on the tensor cores (M >= 6, Nt a multiple of 128): one
 // 128-point tile per CTA.
 template <int M>
-__global__ void __launch_bounds__(kTcRows, 1)
+__global__ void __launch_bounds__(kTcRows, 2)
     mm_contract_adj_tc_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
                               const int* __restrict__ active) {
     extern __shared__ __align__(16) unsigned char tc_smem[];
@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(kTcRows, 1)
 // The adjoint's Im X contraction of FP32-forward batches on the tensor
 // cores (M >= 6, Nt a multiple of 128): one 128-point tile per CTA.
 template <int M>
-__global__ void __launch_bounds__(kTcRows, 1)
+__global__ void __launch_bounds__(kTcRows, 2)
     mm_imx_tc_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
                      const int* __restrict__ active) {
     extern __shared__ __align__(16) unsigned char tc_smem[];
@@ -117,7 +117,7 @@ namespace {
 
 template <int M>
 cudaError_t imx_tc(const MmRound& a) {
-    const size_t smem = TcShape<M>::SMEM;
+    const size_t smem = TcSymShape<M>::SMEM;
     cudaError_t e = cudaFuncSetAttribute(mm_imx_tc_kernel<M>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -129,7 +129,7 @@ cudaError_t imx_tc(const MmRound& a) {
 
 template <int M>
 cudaError_t contract_adj_tc(const MmRound& a) {
-    const size_t smem = TcAdjShape<M>::SMEM_LAUNCH;
+    const size_t smem = TcSymShape<M>::SMEM_LAUNCH;
     cudaError_t e = cudaFuncSetAttribute(mm_contract_adj_tc_kernel<M>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

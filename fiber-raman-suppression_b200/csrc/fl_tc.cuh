@@ -336,32 +336,35 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
 // 3xTF32, while λ, C and the sums over i stay in FP64.  This takes the
 // assembly from about 14 300 FP64 FMAs per time point (10 modes) to 800.
 //
-// B rows hold (i, j) at i*16 + j, so row i of each accumulator is one
-// 16-column tensor-memory load; the three accumulators sit CS columns apart
-// in a 512-column allocation.  Two A buffers: S' and Re w are staged while
-// the MMAs of the other run; Im w reuses the first buffer once its MMAs have
-// completed.  Waits are bounded as in the forward contraction (a timeout
-// sets the tile's outputs to NaN) and tensor memory is freed on every path.
+// G is symmetric in (i, j), so D' and W are too: B holds only the pairs
+// p = (i <= j) (rows padded to 16, the symmetric image), each accumulator
+// is NS <= 64 columns and the three fit a 256-column allocation.  With one
+// A buffer (the three A tiles in turn, each after the previous MMAs have
+// completed) a CTA takes 87 KB of shared memory at M = 10: two CTAs per SM,
+// each one's loads overlapping the other's tensor-core and drain phases.
+// Waits are bounded as in the forward contraction (a timeout sets the
+// tile's outputs to NaN) and tensor memory is freed on every path.
 template <int M>
-struct TcAdjShape {
+struct TcSymShape {
     static constexpr int NP = M * (M + 1) / 2;
     static constexpr int KP = tc_kp(M);
-    static constexpr int NN = 16 * M;                   // MMA N: rows i*16 + j
-    static constexpr int CS = (NN + 31) & ~31;          // columns between accumulators
-    static constexpr int SBO = KP * 32;
+    static constexpr int NS = (NP + 15) & ~15;          // MMA N: the pairs i <= j
+    static constexpr int CS = (NS + 31) & ~31;          // columns between accumulators
     static constexpr int A_BYTES = kTcRows * KP * 4;    // one of A_hi / A_lo
-    static constexpr int B_BYTES = NN * KP * 4;         // one of B_hi / B_lo
-    static constexpr int SMEM = 4 * A_BYTES + 2 * B_BYTES + 64 + 1024;
-    static constexpr uint32_t TMEM_COLS = 512;
-    // launched with at least 116 KB so that one CTA holds an SM and its
-    // 512 tensor-memory columns (no second allocation waits on the first)
-    static constexpr int SMEM_LAUNCH = SMEM > 116 * 1024 ? SMEM : 116 * 1024;
-    static_assert(NN <= 256, "MMA N");
+    static constexpr int B_BYTES = NS * KP * 4;         // one of B_hi / B_lo
+    static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 64 + 1024;
+    // at least 80 KB so that no more than two CTAs (2 x 256 tensor-memory
+    // columns) share an SM: no allocation waits on another CTA's
+    static constexpr int SMEM_LAUNCH = SMEM > 80 * 1024 ? SMEM : 80 * 1024;
+    static constexpr uint32_t TMEM_COLS = 256;
+    static_assert(NS <= 256, "MMA N");
     static_assert(3 * CS <= (int)TMEM_COLS, "accumulator columns");
-    static_assert(SMEM <= 227 * 1024, "shared memory");
+    static_assert(2 * SMEM <= 227 * 1024, "two CTAs per SM");
 };
 
-__host__ __device__ constexpr uint32_t tc_adj_bytes(int M) { return 2u * 16u * M * tc_kp(M) * 4u; }
+__host__ __device__ constexpr uint32_t tc_sym_bytes(int M) {
+    return 2u * (uint32_t)(((M * (M + 1) / 2 + 15) & ~15) * tc_kp(M) * 4);
+}
 
 // bounded wait on an mbarrier phase (true: the phase completed)
 __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, long bound) {
@@ -472,24 +475,22 @@ __device__ __forceinline__ void tc_adj_fill(int op, unsigned char* Ahi, unsigned
 // The adjoint assembly of the 128-point tile `tile` of one slot.
 template <int M>
 __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* smem) {
-    using TS = TcAdjShape<M>;
-    constexpr int NP = TS::NP, KP = TS::KP, NN = TS::NN, CS = TS::CS;
+    using TS = TcSymShape<M>;
+    constexpr int KP = TS::KP, NS = TS::NS, CS = TS::CS;
     static_assert(KP % 4 == 0, "float4 groups");
     const size_t N = (size_t)d.N;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int t = tile * kTcRows + tid;
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
-    unsigned char* Xhi = base;
-    unsigned char* Xlo = Xhi + TS::A_BYTES;
-    unsigned char* Yhi = Xlo + TS::A_BYTES;
-    unsigned char* Ylo = Yhi + TS::A_BYTES;
-    unsigned char* Bhi = Ylo + TS::A_BYTES;
+    unsigned char* Ahi = base;
+    unsigned char* Alo = Ahi + TS::A_BYTES;
+    unsigned char* Bhi = Alo + TS::A_BYTES;
     unsigned char* Blo = Bhi + TS::B_BYTES;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // X MMAs, Y MMAs, B image
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // MMAs, B image
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
     uint32_t* bfail = tmem_slot + 1;
-    const uint32_t barX = smem_u32(bars), barY = smem_u32(bars + 1), barB = smem_u32(bars + 2);
+    const uint32_t barM = smem_u32(bars), barB = smem_u32(bars + 1);
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -501,14 +502,13 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
     static_assert(kBBytes % 16 == 0, "bulk copy size");
     if (tid == 0) {
         *bfail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barX));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barY));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barM));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barB));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
                      "r"(kBBytes)
                      : "memory");
-        const char* src = reinterpret_cast<const char*>(d.Gtca);
+        const char* src = reinterpret_cast<const char*>(d.Gtcs);
         for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
             const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
             asm volatile(
@@ -529,38 +529,34 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
 #pragma unroll
     for (int i = 0; i < M; i++) uf[i] = ut[(size_t)i * N + t];
 
-    // ---- S' into X, then its MMAs (after a bounded wait for the B image)
-    tc_adj_fill<M, KP>(0, Xhi, Xlo, sq, N, t, uf);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
+    // ---- the three A tiles in turn: S' -> columns [0, NS), Re w -> [CS,
+    // CS + NS), Im w -> [2 CS, 2 CS + NS); each refill waits for the MMAs
+    // that read the previous tile (barrier phases 0, 1, 2)
     const uint32_t bh = smem_u32(Bhi), bl = smem_u32(Blo);
-    if (tid == 0) {
-        if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
-        if (!*bfail) tc_issue3<KP, NN>(tmem, smem_u32(Xhi), smem_u32(Xlo), bh, bl);
-        tc_commit(barX);  // arrives once the MMAs above (if any) have completed
+    uint32_t tmem = 0;
+    bool ok = true;
+    int pending = -1;  // parity of a commit whose arrival a timed-out wait did not see
+#pragma unroll 1
+    for (int op = 0; op < 3; op++) {
+        if (op > 0) {  // wait for the previous tile's MMAs (block-uniform outcome)
+            const bool done = tc_wait(barM, (uint32_t)((op - 1) & 1), 1L << 26);
+            if (!done && pending < 0) pending = (op - 1) & 1;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            ok = __syncthreads_and(ok && done ? 1 : 0) != 0;
+            if (!ok) break;
+        }
+        tc_adj_fill<M, KP>(op, Ahi, Alo, sq, N, t, uf);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        tmem = *tmem_slot;
+        if (tid == 0) {
+            if (op == 0 && !tc_wait(barB, 0, 1L << 26)) *bfail = 1;
+            if (!*bfail) tc_issue3<KP, NS>(tmem + (uint32_t)(op * CS), smem_u32(Ahi), smem_u32(Alo), bh, bl);
+            tc_commit(barM);  // arrives once the MMAs above (if any) have completed
+        }
     }
-    // ---- Re w into Y and its MMAs
-    tc_adj_fill<M, KP>(1, Yhi, Ylo, sq, N, t, uf);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (tid == 0) {
-        if (!*bfail) tc_issue3<KP, NN>(tmem + CS, smem_u32(Yhi), smem_u32(Ylo), bh, bl);
-        tc_commit(barY);
-    }
-    // ---- Im w into X once the S' MMAs have read it
-    bool okX = tc_wait(barX, 0, 1L << 26);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (okX) tc_adj_fill<M, KP>(2, Xhi, Xlo, sq, N, t, uf);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    okX = __syncthreads_and(okX ? 1 : 0) != 0;  // block-uniform: a second X commit only if all saw the first
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (tid == 0 && okX) {
-        if (!*bfail) tc_issue3<KP, NN>(tmem + 2 * CS, smem_u32(Xhi), smem_u32(Xlo), bh, bl);
-        tc_commit(barX);
-    }
+
     // ---- η_j = 2i Σ_i C_ij u_i + Σ_i [λ_i D'_ij - (1-fR) conj(λ_i) W_ij]; the
     // FP64 loads and the C term run while the tensor cores finish
     cx<double> la[M];
@@ -591,27 +587,38 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
             }
         }
     }
-    const bool okY = tc_wait(barY, 0, 1L << 26);
-    const bool okX2 = okX && tc_wait(barX, 1, 1L << 26);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool ok = __syncthreads_and((okY && okX2) ? 1 : 0) != 0 && !*bfail;
+    if (ok) {  // the last tile's MMAs (phase 0 again: the fourth use)
+        const bool done = tc_wait(barM, 0, 1L << 26);
+        if (!done && pending < 0) pending = 0;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        ok = __syncthreads_and(done ? 1 : 0) != 0;
+    }
+    ok = ok && !*bfail;
 
     if (ok) {
         const double ofr = d.one_m_fR;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+        float Dv[16], Wr[16], Wi[16];
+        int p = 0;
 #pragma unroll
-        for (int i = 0; i < M; i++) {
-            const cx<double> l = la[i];
-            float Dv[16], Wr[16], Wi[16];
-            tc_ld16(trow + (uint32_t)(i * 16), Dv);
-            tc_ld16(trow + (uint32_t)(CS + i * 16), Wr);
-            tc_ld16(trow + (uint32_t)(2 * CS + i * 16), Wi);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int a = 0; a < M; a++) {
 #pragma unroll
-            for (int j = 0; j < M; j++) {
-                const double dv = Dv[j], wr = Wr[j], wi = Wi[j];
-                er[j] += l.re * dv - ofr * (l.re * wr + l.im * wi);
-                ei[j] += l.im * dv - ofr * (l.re * wi - l.im * wr);
+            for (int b = a; b < M; b++) {
+                if ((p & 15) == 0) {  // the next 16 pairs of each accumulator
+                    tc_ld16(trow + (uint32_t)p, Dv);
+                    tc_ld16(trow + (uint32_t)(CS + p), Wr);
+                    tc_ld16(trow + (uint32_t)(2 * CS + p), Wi);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                }
+                const double dv = Dv[p & 15], wr = Wr[p & 15], wi = Wi[p & 15];
+                // η_b += λ_a D'_ab - (1-fR) conj(λ_a) W_ab, and (a != b) the mirror
+                er[b] += la[a].re * dv - ofr * (la[a].re * wr + la[a].im * wi);
+                ei[b] += la[a].im * dv - ofr * (la[a].re * wi - la[a].im * wr);
+                if (a != b) {
+                    er[a] += la[b].re * dv - ofr * (la[b].re * wr + la[b].im * wi);
+                    ei[a] += la[b].im * dv - ofr * (la[b].re * wi - la[b].im * wr);
+                }
+                p++;
             }
         }
     }
@@ -620,16 +627,12 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
     for (int j = 0; j < M; j++) eta[(size_t)j * N + t] = ok ? mk(er[j], ei[j]) : mk(nan, 0.0);
 
     // ---- cleanup: a B copy that timed out, or MMAs whose completion a
-    // timed-out wait did not see, may still be in flight; wait for them
-    // (bounded) before shared and tensor memory are released
+    // timed-out wait did not see (no MMA was issued after it), may still be
+    // in flight: wait for them (bounded) before shared and tensor memory are
+    // released
     if (tid == 0) {
         if (*bfail) tc_wait(barB, 0, 1L << 26);
-        if (!okX) {
-            tc_wait(barX, 0, 1L << 30);
-        } else if (!okX2) {
-            tc_wait(barX, 1, 1L << 30);
-        }
-        if (!okY) tc_wait(barY, 0, 1L << 30);
+        if (pending >= 0) tc_wait(barM, (uint32_t)pending, 1L << 30);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -642,14 +645,15 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
 // Adjoint first pass of FP32-forward batches (M >= 6) on the tensor cores:
 //   Im X_p = Σ_q G[i,j,q] Y_q  for the pairs p = (i <= j),
 //   Y_q = (Im(λ_k u_l*) + Im(λ_l u_k*))/2 (k < l), Im(λ_k u_k*) (k = l),
-// the forward contraction's GEMM with A = Y (formed in FP64, split 3xTF32)
-// and the forward B image (rows i*M + j); the pairs i <= j of each
-// thread's accumulator row go to C's input table in FP64.  Waits are
-// bounded (a timeout writes NaN) and tensor memory is freed on every path.
+// one GEMM with A = Y (formed in FP64, split 3xTF32) and the symmetric B
+// image (rows p): column p of each thread's accumulator row is Im X_p,
+// stored to C's input table in FP64.  Waits are bounded (a timeout writes
+// NaN) and tensor memory is freed on every path.
 template <int M>
 __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
-    using TS = TcShape<M>;
-    constexpr int KP = TS::KP, NN = TS::NN, NP = TS::NP;
+    using TS = TcSymShape<M>;
+    constexpr int KP = TS::KP, NS = TS::NS, NP = TS::NP;
+    constexpr uint32_t kCols = NS <= 32 ? 32 : NS <= 64 ? 64 : 128;  // allocation: a power of 2 >= 32
     const size_t N = (size_t)d.N;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int t = tile * kTcRows + tid;
@@ -667,7 +671,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(tmem_slot)),
-                     "r"(128));
+                     "r"(kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     constexpr uint32_t kBBytes = 2 * TS::B_BYTES, kBChunk = 16384;
@@ -680,7 +684,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
                      "r"(kBBytes)
                      : "memory");
-        const char* src = reinterpret_cast<const char*>(d.Gtc);
+        const char* src = reinterpret_cast<const char*>(d.Gtcs);
         for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
             const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
             asm volatile(
@@ -712,7 +716,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     const uint32_t tmem = *tmem_slot;
     if (tid == 0) {
         if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
-        if (!*bfail) tc_issue3<KP, NN>(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo));
+        if (!*bfail) tc_issue3<KP, NS>(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo));
         tc_commit(barM);
     }
     const bool done = tc_wait(barM, 0, 1L << 26);
@@ -721,16 +725,13 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     if (ok) {
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
-        for (int c = 0; c < NN; c += 16) {
+        for (int c = 0; c < NS; c += 16) {
             float v[16];
             tc_ld16(trow + (uint32_t)c, v);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int e = 0; e < 16; e++) {
-                const int col = c + e, i = col / M, j = col % M;
-                if (col < M * M && i <= j)
-                    cq[(size_t)(i * M - i * (i - 1) / 2 + (j - i)) * N + t] = (double)v[e];
-            }
+            for (int e = 0; e < 16; e++)
+                if (c + e < NP) cq[(size_t)(c + e) * N + t] = (double)v[e];
         }
     } else {
         const double nan = __longlong_as_double(0x7ff8000000000000LL);
@@ -745,7 +746,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     __syncthreads();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
-                     "r"(128));
+                     "r"(kCols));
 }
 
 }  // namespace fl

@@ -135,7 +135,7 @@ struct MmDesc {
     const void* G[2];       // M*M*GP: G[(i*M + j)*GP + q] (pair q = (k <= l); GP = NP padded to 4)
     const double* Ga;       // NP*M*MP: the same values as Ga[(j*NP + q)*MP + i] (MP = M padded to 2)
     const float* Gtc;       // M >= 6: the tensor-core B operand (G split hi/lo, shared-memory image)
-    const float* Gtca;      // M >= 6: the adjoint's B operand (rows (i, j) at i*16 + j, split hi/lo)
+    const float* Gtcs;      // M >= 6: the symmetric B operand (rows: pairs i <= j, split hi/lo)
     int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
     int adj_mixed;          // mm_adj_mixed(M, N, fp64): mixed-precision adjoint
     int nparts;             // error partial sums per evaluation (M x CTAs per transform)
