@@ -162,6 +162,10 @@ struct fl_problem {
     double* d_Ga = nullptr;                // its adjoint layout
     float* d_Gtc = nullptr;                // its tensor-core operand image (M >= 6)
     float* d_Gtcs = nullptr;               // its symmetric image (pairs i <= j; M >= 6)
+    int rank = 0;                          // low-rank form of the contraction (0: not used)
+    float* d_Vz = nullptr;                 // and its three tensor-core images
+    float* d_Utc = nullptr;
+    float* d_Utcs = nullptr;
     // device staging of the host-buffer batch calls (grow-only, reused)
     char* d_stage = nullptr;
     size_t stage_bytes = 0;
@@ -556,6 +560,10 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         d.Ga = pr->d_Ga;
         d.Gtc = pr->d_Gtc;
         d.Gtcs = pr->d_Gtcs;
+        d.rank = pr->rank;
+        d.Vz = pr->d_Vz;
+        d.Utc = pr->d_Utc;
+        d.Utcs = pr->d_Utcs;
         d.M = pr->m;
         d.nparts = nparts;
         d.NP = w->np;
@@ -760,6 +768,132 @@ __global__ void mm_gather_J_kernel(const MmState* __restrict__ st, int n, double
 // q enumerating k <= l row by row (GP: the pair count padded to 4 with zeros);
 // the adjoint's copy Ga[(j*NP + q)*MP + i] (MP: M padded to 2); γ in the
 // reference's column-major order
+// Eigen-decomposition of a symmetric n x n matrix (row-major; destroyed) by
+// cyclic Jacobi rotations: eigenvalues in w, eigenvectors as the columns of v.
+void sym_eig(std::vector<double>& a, int n, std::vector<double>& w, std::vector<double>& v) {
+    v.assign((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) v[(size_t)i * n + i] = 1.0;
+    double tot = 0.0;
+    for (double x : a) tot += x * x;
+    for (int sweep = 0; sweep < 64; sweep++) {
+        double off = 0.0;
+        for (int p = 0; p < n; p++)
+            for (int q = p + 1; q < n; q++) off += a[(size_t)p * n + q] * a[(size_t)p * n + q];
+        if (off <= 1e-32 * tot) break;
+        for (int p = 0; p < n; p++)
+            for (int q = p + 1; q < n; q++) {
+                const double apq = a[(size_t)p * n + q];
+                if (apq == 0.0) continue;
+                const double th = (a[(size_t)q * n + q] - a[(size_t)p * n + p]) / (2.0 * apq);
+                const double t = (th >= 0.0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+                const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                for (int k = 0; k < n; k++) {  // columns p, q
+                    const double x = a[(size_t)k * n + p], y = a[(size_t)k * n + q];
+                    a[(size_t)k * n + p] = c * x - sn * y;
+                    a[(size_t)k * n + q] = sn * x + c * y;
+                }
+                for (int k = 0; k < n; k++) {  // rows p, q
+                    const double x = a[(size_t)p * n + k], y = a[(size_t)q * n + k];
+                    a[(size_t)p * n + k] = c * x - sn * y;
+                    a[(size_t)q * n + k] = sn * x + c * y;
+                }
+                for (int k = 0; k < n; k++) {
+                    const double x = v[(size_t)k * n + p], y = v[(size_t)k * n + q];
+                    v[(size_t)k * n + p] = c * x - sn * y;
+                    v[(size_t)k * n + q] = sn * x + c * y;
+                }
+            }
+    }
+    w.resize(n);
+    for (int i = 0; i < n; i++) w[i] = a[(size_t)i * n + i];
+}
+
+// TF32 round to nearest of an FP32 value (10-bit mantissa; the tensor cores'
+// operand format), the host side of the 3xTF32 split
+float tf32_host(float x) {
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+
+// A tensor-core B operand image: rows x K (K a multiple of 8, rows a multiple
+// of 8) in the K-major no-swizzle shared-memory layout, split hi then lo.
+template <class F>
+std::vector<unsigned char> tc_image(int rows, int K, F&& f) {
+    const size_t bytes = (size_t)rows * K * 4;
+    std::vector<unsigned char> img(2 * bytes, 0);
+    for (int r = 0; r < rows; r++)
+        for (int k = 0; k < K; k++) {
+            const float g = f(r, k);
+            if (g == 0.f) continue;
+            const float hi = tf32_host(g), lo = tf32_host(g - hi);
+            const uint32_t off = (uint32_t)((r >> 3) * (K * 32) + (k >> 2) * 128 + (r & 7) * 16 + (k & 3) * 4);
+            memcpy(&img[off], &hi, 4);
+            memcpy(&img[bytes + off], &lo, 4);
+        }
+    return img;
+}
+
+int upload_image(fl_ctx* ctx, const std::vector<unsigned char>& img, float** dst) {
+    CU(cudaMalloc(dst, img.size()));
+    CU(cudaMemcpy(*dst, img.data(), img.size(), cudaMemcpyHostToDevice));
+    return FL_OK;
+}
+
+// The low-rank form of the pair contraction (symmetric γ, FP32 batches with
+// M >= 6): the Gram matrix Γ[p][q] = γ_ijkl of the pairs p = (i <= j),
+// q = (k <= l) has rank dim span{φ_i φ_j}, often well below NP (28 of 55 for
+// the ten Hermite-Gauss modes with m + n <= 3, whose products are a Gaussian
+// times the 28 monomials of degree <= 6).  With Γ = Σ_k λ_k Q_k Q_kᵀ over the
+// eigenvalues above 1e-12 of the largest and G[ij][q] = w_q Γ[p][q] (w_q = 2
+// for k < l), every contraction with G factors as
+//   Σ_q G[ij][q] X_q = Σ_k U[p][k] Z_k,  U[p][k] = λ_k Q[p][k],
+//   Z_k = Σ_q V[q][k] X_q,  V[q][k] = w_q Q[q][k],
+// and the FP32 path convolves the r sequences Z_k instead of the NP pair
+// products.  Used when it saves at least one pair transform.
+int mm_lowrank_setup(fl_problem* pr, const double* gamma) {
+    const int M = pr->m, NP = M * (M + 1) / 2, KP = (NP + 7) & ~7;
+    auto g = [&](int i, int j, int k, int l) { return gamma[i + M * (j + M * (k + M * l))]; };
+    std::vector<int> pk(NP), pl(NP);
+    for (int k = 0, q = 0; k < M; k++)
+        for (int l = k; l < M; l++, q++) {
+            pk[q] = k;
+            pl[q] = l;
+        }
+    std::vector<double> Gam((size_t)NP * NP), lam, Q;
+    for (int p = 0; p < NP; p++)
+        for (int q = 0; q < NP; q++) Gam[(size_t)p * NP + q] = g(pk[p], pl[p], pk[q], pl[q]);
+    sym_eig(Gam, NP, lam, Q);
+    std::vector<int> ord(NP);
+    for (int i = 0; i < NP; i++) ord[i] = i;
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return std::fabs(lam[a]) > std::fabs(lam[b]); });
+    const double lmax = std::fabs(lam[ord[0]]);
+    int r = 0;
+    while (r < NP && std::fabs(lam[ord[r]]) > 1e-12 * lmax) r++;
+    // used when it saves pair transforms and the rank fits the kernels' tables
+    if (r == 0 || (r + 1) / 2 >= (NP + 1) / 2 || ((r + 7) & ~7) > mm_krmax(M)) return FL_OK;
+    const int KR = (r + 7) & ~7, NZ = (r + 15) & ~15, NN = (M * M + 15) & ~15, NS = (NP + 15) & ~15;
+    auto U = [&](int p, int k) { return k < r ? (float)(lam[ord[k]] * Q[(size_t)p * NP + ord[k]]) : 0.f; };
+    auto pidx = [&](int i, int j) {
+        const int a = std::min(i, j), b = std::max(i, j);
+        return a * M - a * (a - 1) / 2 + (b - a);
+    };
+    int rc = upload_image(pr->ctx, tc_image(NZ, KP, [&](int k, int q) {
+        return k < r && q < NP ? (float)((pk[q] == pl[q] ? 1.0 : 2.0) * Q[(size_t)q * NP + ord[k]]) : 0.f;
+    }), &pr->d_Vz);
+    if (!rc) rc = upload_image(pr->ctx, tc_image(NN, KR, [&](int row, int k) {
+        return row < M * M ? U(pidx(row / M, row % M), k) : 0.f;
+    }), &pr->d_Utc);
+    if (!rc) rc = upload_image(pr->ctx, tc_image(NS, KR, [&](int p, int k) { return p < NP ? U(p, k) : 0.f; }),
+                               &pr->d_Utcs);
+    if (rc) return rc;
+    pr->rank = r;
+    return FL_OK;
+}
+
 int mm_upload_G(fl_problem* pr, const double* gamma) {
     fl_ctx* ctx = pr->ctx;
     const int M = pr->m, NP = M * (M + 1) / 2, GP = mm_gp(M), MP = mm_mp(M);
@@ -826,6 +960,10 @@ int mm_upload_G(fl_problem* pr, const double* gamma) {
                 }
         CU(cudaMalloc(&pr->d_Gtcs, aimg.size()));
         CU(cudaMemcpy(pr->d_Gtcs, aimg.data(), aimg.size(), cudaMemcpyHostToDevice));
+        if (pr->gamma_sym && mm_adj_mixed(M, pr->nt, pr->precision == FL_PRECISION_FP64)) {
+            const int rc = mm_lowrank_setup(pr, gamma);
+            if (rc) return rc;
+        }
     }
     return FL_OK;
 }
@@ -1159,6 +1297,10 @@ int srv_admit(fl_server* sv, SrvBucket* b, SrvChunk* c, int i, SrvRequest* r) {
         d.Ga = pr->d_Ga;
         d.Gtc = pr->d_Gtc;
         d.Gtcs = pr->d_Gtcs;
+        d.rank = pr->rank;
+        d.Vz = pr->d_Vz;
+        d.Utc = pr->d_Utc;
+        d.Utcs = pr->d_Utcs;
         d.one_m_fR = pr->one_m_fR;
         d.L = r->L;
         d.reltol = pr->reltol;
@@ -1627,6 +1769,9 @@ int fl_problem_destroy(fl_problem* pr) {
     cudaFree(pr->d_Ga);
     cudaFree(pr->d_Gtc);
     cudaFree(pr->d_Gtcs);
+    cudaFree(pr->d_Vz);
+    cudaFree(pr->d_Utc);
+    cudaFree(pr->d_Utcs);
     cudaFree(pr->d_Dturns);
     for (int q = 0; q < 2; q++) {
         cudaFree(pr->d_Heff[q]);

@@ -320,10 +320,14 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     const bool ytask = unit >= ntp;  // correlation of Im X (adjoint only)
     if (ytask && !adj) return;
     if (mixed && ytask != (sizeof(R) == 8)) return;
+    // the low-rank form (rank > 0, FP32 kernels only) convolves pairs of the
+    // rank sequences Z_k = Σ_q V[q][k] P_q instead of the NP products
+    const bool zmode = !ytask && d.rank > 0;
+    const int nseq = zmode ? d.rank : NP;
     const int q0 = 2 * (ytask ? unit - ntp : unit);
-    if (q0 >= NP) return;
+    if (q0 >= nseq) return;
     const int q1 = q0 + 1;
-    const bool two = q1 < NP;
+    const bool two = q1 < nseq;
     G grp;
     grp.init(d, smraw);
     const int tid = grp.g;  // index in the transform group
@@ -343,6 +347,10 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
         if (ytask) {
             p0[s] = cq[(size_t)q0 * N + t];
             p1[s] = two ? cq[(size_t)q1 * N + t] : R(0);
+        } else if (zmode) {
+            const R* zq = sq + (size_t)NP * N;  // Z_k rows (upper half of the pair table)
+            p0[s] = zq[(size_t)q0 * N + t];
+            p1[s] = two ? zq[(size_t)q1 * N + t] : R(0);
         } else {
             const C a = ut[(size_t)k0 * N + t], b = ut[(size_t)l0 * N + t];
             p0[s] = a.re * b.re + a.im * b.im;  // Re(u_k u_l*)

@@ -113,7 +113,34 @@ __global__ void __launch_bounds__(kTcRows, 2)
     mm_imx_tc<M>(d, blockIdx.x, tc_smem);
 }
 
+// The low-rank form's Z reduction (rank > 0): every RHS evaluation of an
+// FP32 batch (forward, and the mixed adjoint's forward field).
+template <int M>
+__global__ void __launch_bounds__(kTcRows, 2)
+    mm_z_tc_kernel(const MmDesc* __restrict__ descs, const MmState* __restrict__ states,
+                   const int* __restrict__ active) {
+    extern __shared__ __align__(16) unsigned char tc_smem[];
+    const int slot = active[blockIdx.y];
+    const MmDesc& d = descs[slot];
+    if (d.M != M || d.rank <= 0 || d.fp64) return;
+    const MmState st = states[slot];
+    if (!mm_rhs_phase(st.phase)) return;
+    mm_z_tc<M>(d, blockIdx.x, tc_smem);
+}
+
 namespace {
+
+template <int M>
+cudaError_t z_tc(const MmRound& a) {
+    const size_t smem = TcShape<M>::SMEM;
+    cudaError_t e = cudaFuncSetAttribute(mm_z_tc_kernel<M>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const dim3 grid(a.N / kTcRows, a.nactive);
+    mm_z_tc_kernel<M><<<grid, kTcRows, smem, a.stream>>>(static_cast<const MmDesc*>(a.desc),
+                                                        a.state, a.active);
+    return cudaGetLastError();
+}
 
 template <int M>
 cudaError_t imx_tc(const MmRound& a) {
@@ -155,6 +182,14 @@ cudaError_t contract_tc(const MmRound& a) {
 
 template <typename R, int M>
 cudaError_t contract_m(const MmRound& a, int which) {
+    // which = 3: the low-rank form's Z reduction (FP32 batches with M >= 6;
+    // slots without a low-rank form skip it)
+    if (which == 3) {
+        if constexpr (M >= 6) {
+            if (mm_adj_mixed(M, a.N, a.fp64)) return z_tc<M>(a);
+        }
+        return cudaSuccess;
+    }
     // FP32 forward with M >= 6 modes: tensor cores (3xTF32)
     if constexpr (sizeof(R) == 4 && M >= 6) {
         if (which == 0 && a.tensor_cores && a.N % kTcRows == 0) return contract_tc<M>(a);

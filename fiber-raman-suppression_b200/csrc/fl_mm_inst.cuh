@@ -59,6 +59,9 @@ cudaError_t mm_round(const MmRound& a) {
     nvtxRangePushA("fl: mm Im X contraction");
     FL_TRY(mm_launch_contract(a, 1));
     nvtxRangePop();
+    nvtxRangePushA("fl: mm low-rank reduction");
+    FL_TRY(mm_launch_contract(a, 3));
+    nvtxRangePop();
     nvtxRangePushA("fl: mm pairs");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 1)));
     FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 1)));

@@ -43,7 +43,7 @@ EvidenceFn mm_evidence_launcher(int logn);
 // evaluation round for Nt = 2^logn (nullptr when not built)
 MmRoundFn mm_round_launcher(int logn);
 // the grid-size-independent kernels (common translation unit)
-cudaError_t mm_launch_contract(const MmRound& a, int which);  // 0 fwd, 1 Im X, 2 adjoint
+cudaError_t mm_launch_contract(const MmRound& a, int which);  // 0 fwd, 1 Im X, 2 adjoint, 3 Z
 cudaError_t mm_launch_control(const MmRound& a, int consume);
 bool mm_supported_modes(int M);
 // CTAs (one cluster) per transform at Nt = 2^logn

@@ -86,6 +86,36 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
 
+// 3 x kp/8 MMAs (3xTF32) of one A tile against B (both kp pairs deep, K-major,
+// split hi/lo) into the accumulator at tmem; n = the MMA's N (rows of B)
+__device__ __forceinline__ void tc_issue3(uint32_t tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
+                                          uint32_t b_lo, int kp, int n) {
+    const uint32_t idesc = tc_idesc(n);
+    const uint32_t sbo = (uint32_t)kp * 32;
+#pragma unroll 1
+    for (int ks = 0; ks < kp / 8; ks++) {
+        const uint32_t koff = (uint32_t)ks * 256;
+        const uint64_t dah = tc_desc(a_hi + koff, 128, sbo);
+        const uint64_t dal = tc_desc(a_lo + koff, 128, sbo);
+        const uint64_t dbh = tc_desc(b_hi + koff, 128, sbo);
+        const uint64_t dbl = tc_desc(b_lo + koff, 128, sbo);
+        const uint32_t acc0 = ks > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+            "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
+    }
+}
+
+
 // The forward contraction of the 128-point tiles t0 = tile*128, tile =
 // first, first + step, ... < N/128 of one slot.  The B operand (the G table,
 // split hi/lo) and the tensor memory are set up once per CTA; each tile
@@ -93,18 +123,22 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
 template <int M>
 __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigned char* smem) {
     using TS = TcShape<M>;
-    constexpr int NP = TS::NP, KP = TS::KP, GP = TS::GP, NN = TS::NN;
+    constexpr int NN = TS::NN;
     const int N = d.N, ntiles = N / kTcRows;
     const int tid = threadIdx.x, warp = tid >> 5;
-    (void)GP;
-    // 1024-byte aligned operand area
+    // K of the GEMM: the pairs, or in the low-rank form the rank (A = S̃_k,
+    // B = U); both padded to whole MMAs of 8
+    const int nk = d.rank > 0 ? d.rank : TS::NP;
+    const int kp = (nk + 7) & ~7;
+    // 1024-byte aligned operand area (laid out for this K; sized for the largest)
     unsigned char* base =
         reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+    const uint32_t a_bytes = (uint32_t)kTcRows * kp * 4, b_bytes = (uint32_t)NN * kp * 4;
     unsigned char* Ahi = base;
-    unsigned char* Alo = Ahi + TS::A_BYTES;
-    unsigned char* Bhi = Alo + TS::A_BYTES;
-    unsigned char* Blo = Bhi + TS::B_BYTES;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // MMA completion
+    unsigned char* Alo = Ahi + a_bytes;
+    unsigned char* Bhi = Alo + a_bytes;
+    unsigned char* Blo = Bhi + b_bytes;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(base + 2 * TS::A_BYTES + 2 * TS::B_BYTES);  // MMA completion
     uint64_t* bbar = mbar + 1;                                         // B-image arrival
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
     uint32_t* bfail = tmem_slot + 1;                                   // B copy timed out
@@ -120,8 +154,7 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
     // problem in exactly this shared-memory layout (B_hi then B_lo), brought in
     // by the TMA engine as bulk copies (16-byte aligned, sizes multiples of 16)
     // completing on bbar, while the threads build the first A tile
-    constexpr uint32_t kBBytes = 2 * TS::B_BYTES, kBChunk = 16384;
-    static_assert(kBBytes % 16 == 0, "bulk copy size");
+    const uint32_t kBBytes = 2 * b_bytes, kBChunk = 16384;  // a multiple of 16 (kp of 8)
     if (tid == 0) {
         *bfail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)));
@@ -131,7 +164,7 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
                          smem_u32(bbar)),
                      "r"(kBBytes)
                      : "memory");
-        const char* src = reinterpret_cast<const char*>(d.Gtc);
+        const char* src = reinterpret_cast<const char*>(d.rank > 0 ? d.Utc : d.Gtc);
         for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
             const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
             asm volatile(
@@ -156,20 +189,20 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
             for (int i = 0; i < M; i++) eta[(size_t)i * N + t] = mk(__int_as_float(0x7fc00000), 0.f);
             continue;
         }
-        // ---- A = this tile's S, split hi/lo: four pairs per 16-byte store
+        // ---- A = this tile's S (or S̃), split hi/lo: four per 16-byte store
 #pragma unroll 2
-        for (int k = 0; k < KP; k += 4) {
+        for (int k = 0; k < kp; k += 4) {
             float4 hi, lo;
             float* h = &hi.x;
             float* l = &lo.x;
 #pragma unroll
             for (int c = 0; c < 4; c++) {
-                const float s = k + c < NP ? sq[(size_t)(k + c) * N + t] : 0.f;
+                const float s = k + c < nk ? sq[(size_t)(k + c) * N + t] : 0.f;
                 h[c] = tf32_rn(s);
                 l[c] = tf32_rn(s - h[c]);
             }
-            *reinterpret_cast<float4*>(Ahi + tc_off<KP>(tid, k)) = hi;
-            *reinterpret_cast<float4*>(Alo + tc_off<KP>(tid, k)) = lo;
+            *reinterpret_cast<float4*>(Ahi + tc_off_rt(tid, k, kp)) = hi;
+            *reinterpret_cast<float4*>(Alo + tc_off_rt(tid, k, kp)) = lo;
         }
         // generic-proxy shared stores -> visible to the tensor core (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -193,32 +226,8 @@ __device__ void mm_contract_fwd_tc(const MmDesc& d, int first, int step, unsigne
             b_waited = true;
             if (!got) *bfail = 1;
         }
-        if (tid == 0 && !*bfail) {
-            constexpr uint32_t idesc = tc_idesc(NN);
-            const uint32_t a_hi = smem_u32(Ahi), a_lo = smem_u32(Alo);
-            const uint32_t b_hi = smem_u32(Bhi), b_lo = smem_u32(Blo);
-#pragma unroll
-            for (int ks = 0; ks < KP / 8; ks++) {
-                const uint32_t koff = (uint32_t)ks * 256;
-                const uint64_t dah = tc_desc(a_hi + koff, 128, TS::SBO);
-                const uint64_t dal = tc_desc(a_lo + koff, 128, TS::SBO);
-                const uint64_t dbh = tc_desc(b_hi + koff, 128, TS::SBO);
-                const uint64_t dbl = tc_desc(b_lo + koff, 128, TS::SBO);
-                const uint32_t acc0 = ks > 0 ? 1u : 0u;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
-            }
-        }
+        if (tid == 0 && !*bfail)
+            tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), kp, NN);
         if (tid == 0)  // arrives once the MMAs above (if any) have completed
             asm volatile(
                 "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -352,7 +361,8 @@ struct TcSymShape {
     static constexpr int CS = (NS + 31) & ~31;          // columns between accumulators
     static constexpr int A_BYTES = kTcRows * KP * 4;    // one of A_hi / A_lo
     static constexpr int B_BYTES = NS * KP * 4;         // one of B_hi / B_lo
-    static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 64 + 1024;
+    static constexpr int U_BYTES = NS * mm_krmax(M) * 4;  // low-rank form: one of U_hi / U_lo
+    static constexpr int SMEM = 2 * A_BYTES + 2 * B_BYTES + 2 * U_BYTES + 64 + 1024;
     // at least 80 KB so that no more than two CTAs (2 x 256 tensor-memory
     // columns) share an SM: no allocation waits on another CTA's
     static constexpr int SMEM_LAUNCH = SMEM > 80 * 1024 ? SMEM : 80 * 1024;
@@ -378,35 +388,6 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, long boun
             : "memory");
     }
     return done != 0;
-}
-
-// 3 x KP/8 MMAs (3xTF32) of one A tile against B into the accumulator at col
-template <int KP, int NN>
-__device__ __forceinline__ void tc_issue3(uint32_t tmem, uint32_t a_hi, uint32_t a_lo, uint32_t b_hi,
-                                          uint32_t b_lo) {
-    constexpr uint32_t idesc = tc_idesc(NN);
-    constexpr uint32_t sbo = KP * 32;
-#pragma unroll
-    for (int ks = 0; ks < KP / 8; ks++) {
-        const uint32_t koff = (uint32_t)ks * 256;
-        const uint64_t dah = tc_desc(a_hi + koff, 128, sbo);
-        const uint64_t dal = tc_desc(a_lo + koff, 128, sbo);
-        const uint64_t dbh = tc_desc(b_hi + koff, 128, sbo);
-        const uint64_t dbl = tc_desc(b_lo + koff, 128, sbo);
-        const uint32_t acc0 = ks > 0 ? 1u : 0u;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-            "l"(dah), "l"(dbh), "r"(idesc), "r"(acc0));
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-            "l"(dah), "l"(dbl), "r"(idesc), "r"(1u));
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-            "l"(dal), "l"(dbh), "r"(idesc), "r"(1u));
-    }
 }
 
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
@@ -487,10 +468,15 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
     unsigned char* Alo = Ahi + TS::A_BYTES;
     unsigned char* Bhi = Alo + TS::A_BYTES;
     unsigned char* Blo = Bhi + TS::B_BYTES;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // MMAs, B image
+    unsigned char* Uhi = Blo + TS::B_BYTES;  // low-rank form: U (rows p, kr deep)
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Uhi + 2 * TS::U_BYTES);  // MMAs, B images
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
     uint32_t* bfail = tmem_slot + 1;
     const uint32_t barM = smem_u32(bars), barB = smem_u32(bars + 1);
+    // the low-rank form takes D' = U S̃' (K = the rank, padded to 8)
+    const int kr = d.rank > 0 ? (d.rank + 7) & ~7 : 0;
+    const uint32_t u_bytes = (uint32_t)NS * kr * 4;
+    unsigned char* Ulo = Uhi + u_bytes;
 
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -506,16 +492,20 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barB));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
-                     "r"(kBBytes)
+                     "r"(kBBytes + 2 * u_bytes)
                      : "memory");
-        const char* src = reinterpret_cast<const char*>(d.Gtcs);
-        for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
-            const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
-            asm volatile(
-                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
-                "[%3];" ::"r"(smem_u32(Bhi) + off),
-                "l"(src + off), "r"(n), "r"(barB)
-                : "memory");
+        for (int img = 0; img < 2; img++) {  // G (symmetric), then U if used
+            const char* src = reinterpret_cast<const char*>(img == 0 ? d.Gtcs : d.Utcs);
+            const uint32_t bytes = img == 0 ? kBBytes : 2 * u_bytes;  // multiples of 16
+            const uint32_t dst = smem_u32(img == 0 ? Bhi : Uhi);
+            for (uint32_t off = 0; off < bytes; off += kBChunk) {
+                const uint32_t n = bytes - off < kBChunk ? bytes - off : kBChunk;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
+                    "%2, [%3];" ::"r"(dst + off),
+                    "l"(src + off), "r"(n), "r"(barB)
+                    : "memory");
+            }
         }
     }
 
@@ -545,14 +535,38 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
             ok = __syncthreads_and(ok && done ? 1 : 0) != 0;
             if (!ok) break;
         }
-        tc_adj_fill<M, KP>(op, Ahi, Alo, sq, N, t, uf);
+        const bool lowrank = op == 0 && kr > 0;
+        if (lowrank) {
+            // A = S̃'_k (k < rank), kr deep
+#pragma unroll 2
+            for (int k = 0; k < kr; k += 4) {
+                float4 hi, lo;
+                float* h = &hi.x;
+                float* l = &lo.x;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const float x = k + c < d.rank ? sq[(size_t)(k + c) * N + t] : 0.f;
+                    h[c] = tf32_rn(x);
+                    l[c] = tf32_rn(x - h[c]);
+                }
+                *reinterpret_cast<float4*>(Ahi + tc_off_rt(tid, k, kr)) = hi;
+                *reinterpret_cast<float4*>(Alo + tc_off_rt(tid, k, kr)) = lo;
+            }
+        } else {
+            tc_adj_fill<M, KP>(op, Ahi, Alo, sq, N, t, uf);
+        }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         tmem = *tmem_slot;
         if (tid == 0) {
             if (op == 0 && !tc_wait(barB, 0, 1L << 26)) *bfail = 1;
-            if (!*bfail) tc_issue3<KP, NS>(tmem + (uint32_t)(op * CS), smem_u32(Ahi), smem_u32(Alo), bh, bl);
+            if (!*bfail) {
+                if (lowrank)
+                    tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Uhi), smem_u32(Ulo), kr, NS);
+                else
+                    tc_issue3(tmem + (uint32_t)(op * CS), smem_u32(Ahi), smem_u32(Alo), bh, bl, KP, NS);
+            }
             tc_commit(barM);  // arrives once the MMAs above (if any) have completed
         }
     }
@@ -716,7 +730,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     const uint32_t tmem = *tmem_slot;
     if (tid == 0) {
         if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
-        if (!*bfail) tc_issue3<KP, NS>(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo));
+        if (!*bfail) tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), KP, NS);
         tc_commit(barM);
     }
     const bool done = tc_wait(barM, 0, 1L << 26);
@@ -737,6 +751,107 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
         const double nan = __longlong_as_double(0x7ff8000000000000LL);
 #pragma unroll 1
         for (int p = 0; p < NP; p++) cq[(size_t)p * N + t] = nan;
+    }
+    if (tid == 0) {
+        if (*bfail) tc_wait(barB, 0, 1L << 26);
+        if (!done) tc_wait(barM, 0, 1L << 30);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(*tmem_slot),
+                     "r"(kCols));
+}
+
+// ---------------------------------------------------------------------------
+// The low-rank form's reduction (rank > 0): Z_k = Σ_q V[q][k] P_q over the
+// pair products P_q = Re(u_k' u_l'*) of the FP32 forward field, for the
+// forward and the mixed adjoint alike, one GEMM per 128-point tile with A = P
+// (split 3xTF32) and B = the V image (rows k, the rank padded to 16).  The
+// pair transforms then convolve the Z_k (upper half of the pair table, FP32
+// rows) instead of the NP products.  Waits are bounded (a timeout writes NaN)
+// and tensor memory is freed on every path.
+template <int M>
+__device__ void mm_z_tc(const MmDesc& d, int tile, unsigned char* smem) {
+    using TS = TcShape<M>;
+    constexpr int KP = TS::KP, NP = TS::NP;
+    constexpr uint32_t kCols = 64;  // >= the rank padded to 16 (mm_krmax(10) = 32)
+    static_assert(mm_krmax(M) + 16 <= (int)kCols, "Z accumulator columns");
+    const size_t N = (size_t)d.N;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int t = tile * kTcRows + tid;
+    const int r = d.rank, nz = (r + 15) & ~15;
+    unsigned char* base =
+        reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem) + 1023) & ~uintptr_t(1023));
+    unsigned char* Ahi = base;
+    unsigned char* Alo = Ahi + TS::A_BYTES;
+    unsigned char* Bhi = Alo + TS::A_BYTES;
+    const uint32_t b_bytes = (uint32_t)nz * KP * 4;
+    unsigned char* Blo = Bhi + b_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Bhi + 2 * TS::B_BYTES);  // MMAs, B image
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    uint32_t* bfail = tmem_slot + 1;
+    const uint32_t barM = smem_u32(bars), barB = smem_u32(bars + 1);
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(kCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    const uint32_t kBBytes = 2 * b_bytes, kBChunk = 16384;  // a multiple of 16
+    if (tid == 0) {
+        *bfail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barM));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barB));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
+                     "r"(kBBytes)
+                     : "memory");
+        const char* src = reinterpret_cast<const char*>(d.Vz);
+        for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
+            const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+                "[%3];" ::"r"(smem_u32(Bhi) + off),
+                "l"(src + off), "r"(n), "r"(barB)
+                : "memory");
+        }
+    }
+    const cx<float>* ut = static_cast<const cx<float>*>(d.ut);
+    float* zq = static_cast<float*>(d.sq) + (size_t)NP * N;  // upper half of the pair table
+    cx<float> u[M];
+#pragma unroll
+    for (int i = 0; i < M; i++) u[i] = ut[(size_t)i * N + t];
+    tc_fill_pairs<M, KP>(Ahi, Alo, [&](int, int k, int l) -> float {
+        return u[k].re * u[l].re + u[k].im * u[l].im;  // Re(u_k u_l*)
+    });
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    if (tid == 0) {
+        if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
+        if (!*bfail) tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), KP, nz);
+        tc_commit(barM);
+    }
+    const bool done = tc_wait(barM, 0, 1L << 26);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const bool ok = __syncthreads_and(done ? 1 : 0) != 0 && !*bfail;
+    if (ok) {
+        const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < nz; c += 16) {
+            float v[16];
+            tc_ld16(trow + (uint32_t)c, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 16; e++)
+                if (c + e < r) zq[(size_t)(c + e) * N + t] = v[e];
+        }
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < r; k++) zq[(size_t)k * N + t] = __int_as_float(0x7fc00000);
     }
     if (tid == 0) {
         if (*bfail) tc_wait(barB, 0, 1L << 26);

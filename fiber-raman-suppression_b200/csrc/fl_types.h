@@ -116,6 +116,10 @@ __host__ __device__ constexpr int mm_mp(int M) { return (M + 1) & ~1; }
 // tiles runs mixed: λ and everything linear in it in FP64, while the forward
 // field's transform and pair products (known to FP32 accuracy) run in FP32
 // and the contractions on the tensor cores (3xTF32).
+// the largest K (rank padded to 8) of the low-rank form: half the pair depth
+__host__ __device__ constexpr int mm_krmax(int M) {
+    return ((((M * (M + 1) / 2 + 7) & ~7) / 2) + 7) & ~7;
+}
 __host__ __device__ constexpr bool mm_adj_mixed(int M, int N, int fp64) {
     return !fp64 && M >= 6 && N % 128 == 0;
 }
@@ -136,6 +140,12 @@ struct MmDesc {
     const double* Ga;       // NP*M*MP: the same values as Ga[(j*NP + q)*MP + i] (MP = M padded to 2)
     const float* Gtc;       // M >= 6: the tensor-core B operand (G split hi/lo, shared-memory image)
     const float* Gtcs;      // M >= 6: the symmetric B operand (rows: pairs i <= j, split hi/lo)
+    // low-rank form of the pair contraction (rank > 0; FP32 batches, M >= 6):
+    // Σ_q G[ij][q] X_q = Σ_k U[ij][k] Z_k with Z_k = Σ_q V[q][k] X_q, k < rank
+    int rank;
+    const float* Vz;        // B of the Z GEMM: rows k (rank padded to 16), K = pairs, V[q][k]
+    const float* Utc;       // B of the forward contraction: rows ij, K = k (rank padded to 8)
+    const float* Utcs;      // B of the adjoint's D': rows p = (i <= j), K = k
     int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
     int adj_mixed;          // mm_adj_mixed(M, N, fp64): mixed-precision adjoint
     int nparts;             // error partial sums per evaluation (M x CTAs per transform)
