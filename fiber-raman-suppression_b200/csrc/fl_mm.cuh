@@ -322,8 +322,9 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
     if (mixed && ytask != (sizeof(R) == 8)) return;
     // the low-rank form (rank > 0, FP32 kernels only) convolves pairs of the
     // rank sequences Z_k = Σ_q V[q][k] P_q instead of the NP products
+    // (and the adjoint correlates the rank sequences Yz_k = Σ_q V[q][k] Y_q)
     const bool zmode = !ytask && d.rank > 0;
-    const int nseq = zmode ? d.rank : NP;
+    const int nseq = d.rank > 0 ? d.rank : NP;
     const int q0 = 2 * (ytask ? unit - ntp : unit);
     if (q0 >= nseq) return;
     const int q1 = q0 + 1;

@@ -368,7 +368,7 @@ struct TcSymShape {
     static constexpr int SMEM_LAUNCH = SMEM > 80 * 1024 ? SMEM : 80 * 1024;
     static constexpr uint32_t TMEM_COLS = 256;
     static_assert(NS <= 256, "MMA N");
-    static_assert(3 * CS <= (int)TMEM_COLS, "accumulator columns");
+    static_assert(4 * CS <= (int)TMEM_COLS, "accumulator columns (four in the low-rank form)");
     static_assert(2 * SMEM <= 227 * 1024, "two CTAs per SM");
 };
 
@@ -519,15 +519,17 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
 #pragma unroll
     for (int i = 0; i < M; i++) uf[i] = ut[(size_t)i * N + t];
 
-    // ---- the three A tiles in turn: S' -> columns [0, NS), Re w -> [CS,
-    // CS + NS), Im w -> [2 CS, 2 CS + NS); each refill waits for the MMAs
-    // that read the previous tile (barrier phases 0, 1, 2)
+    // ---- the A tiles in turn: S' (or S̃') -> columns [0, NS), Re w -> [CS,
+    // CS + NS), Im w -> [2 CS, 2 CS + NS) and, in the low-rank form, the
+    // correlations Cz -> [3 CS, 3 CS + NS) (C = U Cz); each refill waits for
+    // the MMAs that read the previous tile (barrier phases 0, 1, 0, 1)
     const uint32_t bh = smem_u32(Bhi), bl = smem_u32(Blo);
+    const int nops = kr > 0 ? 4 : 3;
     uint32_t tmem = 0;
     bool ok = true;
     int pending = -1;  // parity of a commit whose arrival a timed-out wait did not see
 #pragma unroll 1
-    for (int op = 0; op < 3; op++) {
+    for (int op = 0; op < nops; op++) {
         if (op > 0) {  // wait for the previous tile's MMAs (block-uniform outcome)
             const bool done = tc_wait(barM, (uint32_t)((op - 1) & 1), 1L << 26);
             if (!done && pending < 0) pending = (op - 1) & 1;
@@ -535,9 +537,9 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
             ok = __syncthreads_and(ok && done ? 1 : 0) != 0;
             if (!ok) break;
         }
-        const bool lowrank = op == 0 && kr > 0;
+        const bool lowrank = (op == 0 || op == 3) && kr > 0;
         if (lowrank) {
-            // A = S̃'_k (k < rank), kr deep
+            // A = S̃'_k or Cz_k (k < rank), kr deep
 #pragma unroll 2
             for (int k = 0; k < kr; k += 4) {
                 float4 hi, lo;
@@ -545,7 +547,9 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
                 float* l = &lo.x;
 #pragma unroll
                 for (int c = 0; c < 4; c++) {
-                    const float x = k + c < d.rank ? sq[(size_t)(k + c) * N + t] : 0.f;
+                    const float x = k + c >= d.rank ? 0.f
+                                    : op == 0       ? sq[(size_t)(k + c) * N + t]
+                                                    : (float)cq[(size_t)(k + c) * N + t];
                     h[c] = tf32_rn(x);
                     l[c] = tf32_rn(x - h[c]);
                 }
@@ -563,7 +567,8 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
             if (op == 0 && !tc_wait(barB, 0, 1L << 26)) *bfail = 1;
             if (!*bfail) {
                 if (lowrank)
-                    tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Uhi), smem_u32(Ulo), kr, NS);
+                    tc_issue3(tmem + (uint32_t)(op * CS), smem_u32(Ahi), smem_u32(Alo), smem_u32(Uhi),
+                              smem_u32(Ulo), kr, NS);
                 else
                     tc_issue3(tmem + (uint32_t)(op * CS), smem_u32(Ahi), smem_u32(Alo), bh, bl, KP, NS);
             }
@@ -585,25 +590,28 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
             er[i] = 0.0;
             ei[i] = 0.0;
         }
-        int p = 0;
+        if (kr == 0) {  // (the low-rank form reads C from tensor memory below)
+            int p = 0;
 #pragma unroll
-        for (int a = 0; a < M; a++) {
+            for (int a = 0; a < M; a++) {
 #pragma unroll
-            for (int b = a; b < M; b++) {
-                const double c2 = 2.0 * cq[(size_t)p * N + t];
-                er[b] -= c2 * u[a].im;
-                ei[b] += c2 * u[a].re;
-                if (a != b) {
-                    er[a] -= c2 * u[b].im;
-                    ei[a] += c2 * u[b].re;
+                for (int b = a; b < M; b++) {
+                    const double c2 = 2.0 * cq[(size_t)p * N + t];
+                    er[b] -= c2 * u[a].im;
+                    ei[b] += c2 * u[a].re;
+                    if (a != b) {
+                        er[a] -= c2 * u[b].im;
+                        ei[a] += c2 * u[b].re;
+                    }
+                    p++;
                 }
-                p++;
             }
         }
     }
-    if (ok) {  // the last tile's MMAs (phase 0 again: the fourth use)
-        const bool done = tc_wait(barM, 0, 1L << 26);
-        if (!done && pending < 0) pending = 0;
+    if (ok) {  // the last tile's MMAs
+        const uint32_t par = (uint32_t)((nops - 1) & 1);
+        const bool done = tc_wait(barM, par, 1L << 26);
+        if (!done && pending < 0) pending = (int)par;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         ok = __syncthreads_and(done ? 1 : 0) != 0;
     }
@@ -612,7 +620,7 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
     if (ok) {
         const double ofr = d.one_m_fR;
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-        float Dv[16], Wr[16], Wi[16];
+        float Dv[16], Wr[16], Wi[16], Cv[16];
         int p = 0;
 #pragma unroll
         for (int a = 0; a < M; a++) {
@@ -622,7 +630,17 @@ __device__ void mm_contract_adj_tc(const MmDesc& d, int tile, unsigned char* sme
                     tc_ld16(trow + (uint32_t)p, Dv);
                     tc_ld16(trow + (uint32_t)(CS + p), Wr);
                     tc_ld16(trow + (uint32_t)(2 * CS + p), Wi);
+                    if (kr > 0) tc_ld16(trow + (uint32_t)(3 * CS + p), Cv);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                }
+                if (kr > 0) {  // 2i C_ab u_a into η_b (and the mirror)
+                    const double c2 = 2.0 * (double)Cv[p & 15];
+                    er[b] -= c2 * (double)uf[a].im;
+                    ei[b] += c2 * (double)uf[a].re;
+                    if (a != b) {
+                        er[a] -= c2 * (double)uf[b].im;
+                        ei[a] += c2 * (double)uf[b].re;
+                    }
                 }
                 const double dv = Dv[p & 15], wr = Wr[p & 15], wi = Wi[p & 15];
                 // η_b += λ_a D'_ab - (1-fR) conj(λ_a) W_ab, and (a != b) the mirror
@@ -676,8 +694,13 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     unsigned char* Ahi = base;
     unsigned char* Alo = Ahi + TS::A_BYTES;
     unsigned char* Bhi = Alo + TS::A_BYTES;
-    unsigned char* Blo = Bhi + TS::B_BYTES;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(Blo + TS::B_BYTES);  // MMAs, B image
+    // the low-rank form reduces Y to the rank instead: Yz_k = Σ_q V[q][k] Y_q
+    // (B = the V image, rows k), whose correlations the pair kernel takes
+    const bool lr = d.rank > 0;
+    const int nb = lr ? (d.rank + 15) & ~15 : NS, nout = lr ? d.rank : NP;
+    const uint32_t b_bytes = (uint32_t)nb * KP * 4;
+    unsigned char* Blo = Bhi + b_bytes;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Bhi + 2 * TS::B_BYTES);  // MMAs, B image
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
     uint32_t* bfail = tmem_slot + 1;
     const uint32_t barM = smem_u32(bars), barB = smem_u32(bars + 1);
@@ -688,8 +711,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
                      "r"(kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    constexpr uint32_t kBBytes = 2 * TS::B_BYTES, kBChunk = 16384;
-    static_assert(kBBytes % 16 == 0, "bulk copy size");
+    const uint32_t kBBytes = 2 * b_bytes, kBChunk = 16384;  // a multiple of 16
     if (tid == 0) {
         *bfail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(barM));
@@ -698,7 +720,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(barB),
                      "r"(kBBytes)
                      : "memory");
-        const char* src = reinterpret_cast<const char*>(d.Gtcs);
+        const char* src = reinterpret_cast<const char*>(lr ? d.Vz : d.Gtcs);
         for (uint32_t off = 0; off < kBBytes; off += kBChunk) {
             const uint32_t n = kBBytes - off < kBChunk ? kBBytes - off : kBChunk;
             asm volatile(
@@ -730,7 +752,7 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     const uint32_t tmem = *tmem_slot;
     if (tid == 0) {
         if (!tc_wait(barB, 0, 1L << 26)) *bfail = 1;
-        if (!*bfail) tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), KP, NS);
+        if (!*bfail) tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), KP, nb);
         tc_commit(barM);
     }
     const bool done = tc_wait(barM, 0, 1L << 26);
@@ -738,19 +760,19 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
     const bool ok = __syncthreads_and(done ? 1 : 0) != 0 && !*bfail;
     if (ok) {
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-        for (int c = 0; c < NS; c += 16) {
+#pragma unroll 1
+        for (int c = 0; c < nb; c += 16) {
             float v[16];
             tc_ld16(trow + (uint32_t)c, v);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
             for (int e = 0; e < 16; e++)
-                if (c + e < NP) cq[(size_t)(c + e) * N + t] = (double)v[e];
+                if (c + e < nout) cq[(size_t)(c + e) * N + t] = (double)v[e];
         }
     } else {
         const double nan = __longlong_as_double(0x7ff8000000000000LL);
 #pragma unroll 1
-        for (int p = 0; p < NP; p++) cq[(size_t)p * N + t] = nan;
+        for (int p = 0; p < nout; p++) cq[(size_t)p * N + t] = nan;
     }
     if (tid == 0) {
         if (*bfail) tc_wait(barB, 0, 1L << 26);
