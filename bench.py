@@ -391,12 +391,19 @@ def multimode_measure(ctx, dev, B, steps, warmup):
     # roofline bytes per attempted step: 336 N M (forward and recompute), 384 N M (adjoint)
     alg_bytes = (BYTES_FWD_STEP * (fwd_att + rec) + BYTES_ADJ_STEP * adj_att) * N * M
     peak, peak_kind = measured_peak()
-    # tensor-pipe work on tcgen05 kind::tf32, 6 RHS per attempted step: the FP32
-    # forward contraction, 2 M^4 N flops per forward RHS (forward and recompute),
-    # and the mixed adjoint's four pair-by-pair GEMMs (Im X; D' = G S', G Re w,
-    # G Im w), 4 * 2 NP^2 N flops per adjoint RHS (NP = M(M+1)/2, unpadded)
+    # tensor-pipe work on tcgen05 kind::tf32 (unpadded GEMM flops, 6 RHS per
+    # attempted step), with the rank r of the overlap Gram matrix (the library
+    # drops eigenvalues below 1e-12 of the largest): per forward RHS the
+    # reduction Z = Vᵀ P (2 NP r N) and the contraction U S̃ over all M² rows
+    # (2 M² r N); per adjoint RHS the reductions of Y, D' = U S̃', C = U Cz
+    # (2 NP r N each) and W = G w (2 * 2 NP² N)
     NP = M * (M + 1) // 2
-    tc_flops = 2 * M ** 4 * N * 6 * (fwd_att + rec) + 8 * NP ** 2 * N * 6 * adj_att
+    pairs = [(k, l) for k in range(M) for l in range(k, M)]
+    gam = np.array([[fp.gamma[i, j, k, l] for (k, l) in pairs] for (i, j) in pairs])
+    ev = np.abs(np.linalg.eigvalsh(gam))
+    r = int(np.sum(ev > 1e-12 * ev.max()))
+    tc_flops = ((2 * NP * r + 2 * M * M * r) * N * 6 * (fwd_att + rec)
+                + (3 * 2 * NP * r + 4 * NP * NP) * N * 6 * adj_att)
     out["config4"] = {
         "workload": f"config 4: M=10 HG(m+n<=3), Nt=2^14 over 10 ps, L=2 m, 5 nJ, {B} per-mode "
                     "phase candidates N(0,1), fwd+adjoint, 160 dense-output steps",
@@ -409,13 +416,15 @@ def multimode_measure(ctx, dev, B, steps, warmup):
                      "scope": "whole batch (all multimode kernels) over its call time"},
         "tensor": {"flops_per_batch": tc_flops,
                    "achieved_tflops_over_batch": tc_flops / t_batch / 1e12,
-                   "note": "forward contraction and the adjoint's Im X and D'/W GEMMs "
-                           "(algorithmic flops); 3 tf32 MMAs per product (3xTF32 split)"},
+                   "gram_rank": r,
+                   "note": "the low-rank reductions and contractions and the adjoint's W GEMMs "
+                           "(unpadded flops); 3 tf32 MMAs per product (3xTF32 split)"},
         "precision": "FP32 forward; mixed adjoint: lambda, its transforms and the sums over "
                      "modes FP64, the forward field's transform and pair products FP32, "
                      "per-point contractions 3xTF32",
-        "contraction": "tcgen05 kind::tf32 (3xTF32): the forward contraction, the adjoint's "
-                       "Im X and D' = G S', W = G u_k u_l on the symmetric pair image"}
+        "contraction": "tcgen05 kind::tf32 (3xTF32), low-rank form G = U V^T of the overlap "
+                       "Gram matrix: Z = V^T P, D = U S~, the adjoint's D', C = U Cz and "
+                       "W = G u_k u_l on the symmetric pair image"}
     fp2 = P.multimode_problem(2, 64, 4096, 5.0, 1.0, 2e-9, 200e-15, seed=0,
                               raman_threshold_thz=-2.0)
     gp2 = GPUProblem(ctx, fp2)
