@@ -2260,8 +2260,32 @@ static int phase_gradient_host(fl_problem* pr, const double* u0, int nbatch,
     bool any = false;
     for (int i = 0; i < nt; i++) any |= mask[i] != 0;
     if (!any) return set_err(ctx, FL_EINVAL, "band mask must contain at least one bin");
-    for (size_t i = 0; i < np; i++)
-        if (!std::isfinite(phases[i])) return set_err(ctx, FL_EINVAL, "phase values must be finite");
+    // every phase must be finite: a large batch is scanned on a host thread
+    // while the GPU runs it (the scan reads the whole input once, several ms
+    // at 592 x 2^13 values); a call with a non-finite phase still returns
+    // FL_EINVAL and writes no output
+    auto nonfinite = [phases](size_t lo, size_t hi) {
+        uint64_t bad = 0;
+        for (size_t i = lo; i < hi; i++) {
+            uint64_t b;
+            memcpy(&b, &phases[i], 8);
+            bad |= (uint64_t)(((b >> 52) & 0x7ff) == 0x7ff);
+        }
+        return bad != 0;
+    };
+    bool bad_phase = false;
+    std::thread scan;
+    if (np < ((size_t)1 << 20)) {
+        if (nonfinite(0, np)) return set_err(ctx, FL_EINVAL, "phase values must be finite");
+    } else {
+        scan = std::thread([&] { bad_phase = nonfinite(0, np); });
+    }
+    struct Join {
+        std::thread& t;
+        ~Join() {
+            if (t.joinable()) t.join();
+        }
+    } join_scan{scan};
     if (cudaSetDevice(ctx->device) != cudaSuccess) return set_err(ctx, FL_ENODEV, "cudaSetDevice");
     // inputs and outputs in the problem's staging area: one allocation that
     // grows to the largest batch seen and is reused by later calls
@@ -2289,6 +2313,11 @@ static int phase_gradient_host(fl_problem* pr, const double* u0, int nbatch,
     CU(cudaMemcpyAsync(d_ph, phases, 8 * np, cudaMemcpyHostToDevice, ctx->stream));
     CU(cudaMemcpyAsync(d_m, mask, nt, cudaMemcpyHostToDevice, ctx->stream));
     rc = phase_gradient_device(pr, d_u0, nbatch, d_ph, per_mode, d_m, log_cost, d_J, d_g, stats);
+    if (scan.joinable()) scan.join();
+    if (bad_phase) {
+        CU(cudaStreamSynchronize(ctx->stream));
+        return set_err(ctx, FL_EINVAL, "phase values must be finite");
+    }
     if (rc == FL_OK) {
         CU(cudaMemcpyAsync(J, d_J, 8 * (size_t)nbatch, cudaMemcpyDeviceToHost, ctx->stream));
         CU(cudaMemcpyAsync(grad, d_g, 8 * np, cudaMemcpyDeviceToHost, ctx->stream));

@@ -107,7 +107,8 @@ __global__ void __launch_bounds__(kTcRows, 2)
     extern __shared__ __align__(16) unsigned char tc_smem[];
     const int slot = active[blockIdx.y];
     const MmDesc& d = descs[slot];
-    if (d.M != M || !d.adj_mixed) return;
+    // (with a low-rank form the Z kernel reduces Y to the rank instead)
+    if (d.M != M || !d.adj_mixed || d.rank > 0) return;
     const MmState st = states[slot];
     if (!mm_takes<double>(d, st) || !mm_adjoint_phase(st.phase)) return;
     mm_imx_tc<M>(d, blockIdx.x, tc_smem);
@@ -125,7 +126,7 @@ __global__ void __launch_bounds__(kTcRows, 2)
     if (d.M != M || d.rank <= 0 || d.fp64) return;
     const MmState st = states[slot];
     if (!mm_rhs_phase(st.phase)) return;
-    mm_z_tc<M>(d, blockIdx.x, tc_smem);
+    mm_z_tc<M>(d, blockIdx.x, tc_smem, mm_adjoint_phase(st.phase));
 }
 
 namespace {

@@ -791,14 +791,16 @@ __device__ void mm_imx_tc(const MmDesc& d, int tile, unsigned char* smem) {
 // forward and the mixed adjoint alike, one GEMM per 128-point tile with A = P
 // (split 3xTF32) and B = the V image (rows k, the rank padded to 16).  The
 // pair transforms then convolve the Z_k (upper half of the pair table, FP32
-// rows) instead of the NP products.  Waits are bounded (a timeout writes NaN)
-// and tensor memory is freed on every path.
+// rows) instead of the NP products.  In the adjoint the same kernel reduces
+// Y (the Im X inputs) to the rank with a second GEMM on the same image.
+// Waits are bounded (a timeout writes NaN) and tensor memory is freed on
+// every path.
 template <int M>
-__device__ void mm_z_tc(const MmDesc& d, int tile, unsigned char* smem) {
+__device__ void mm_z_tc(const MmDesc& d, int tile, unsigned char* smem, bool adj) {
     using TS = TcShape<M>;
     constexpr int KP = TS::KP, NP = TS::NP;
-    constexpr uint32_t kCols = 64;  // >= the rank padded to 16 (mm_krmax(10) = 32)
-    static_assert(mm_krmax(M) + 16 <= (int)kCols, "Z accumulator columns");
+    constexpr uint32_t kCols = 64;  // Z in [0, 32), the adjoint's Yz in [32, 64)
+    static_assert(((mm_krmax(M) + 15) & ~15) <= 32, "Z accumulator columns");
     const size_t N = (size_t)d.N;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int t = tile * kTcRows + tid;
@@ -857,9 +859,39 @@ __device__ void mm_z_tc(const MmDesc& d, int tile, unsigned char* smem) {
         if (!*bfail) tc_issue3(tmem, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), KP, nz);
         tc_commit(barM);
     }
-    const bool done = tc_wait(barM, 0, 1L << 26);
+    bool done = tc_wait(barM, 0, 1L << 26);
+    int pending = done ? -1 : 0;  // parity of a commit whose arrival a timed-out wait did not see
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const bool ok = __syncthreads_and(done ? 1 : 0) != 0 && !*bfail;
+    bool ok = __syncthreads_and(done ? 1 : 0) != 0;
+    // the adjoint also reduces Y_q = (Im(λ_k u_l*) + Im(λ_l u_k*))/2 (k < l),
+    // Im(λ_k u_k*) (k = l) to Yz_k = Σ_q V[q][k] Y_q (columns [32, 32 + nz)),
+    // whose correlations the FP64 pair kernel takes (C = U Cz)
+    if (adj && ok) {
+        const cx<double>* lt = static_cast<const cx<double>*>(d.lt);
+        cx<double> la[M];
+#pragma unroll
+        for (int i = 0; i < M; i++) la[i] = lt[(size_t)i * N + t];
+        tc_fill_pairs<M, KP>(Ahi, Alo, [&](int, int k, int l) -> float {
+            const double a = la[k].im * (double)u[l].re - la[k].re * (double)u[l].im;  // Im(λ_k u_l*)
+            if (k == l) return (float)a;
+            const double b = la[l].im * (double)u[k].re - la[l].re * (double)u[k].im;
+            return (float)(0.5 * (a + b));
+        });
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) {
+            if (!*bfail)
+                tc_issue3(tmem + 32, smem_u32(Ahi), smem_u32(Alo), smem_u32(Bhi), smem_u32(Blo), KP, nz);
+            tc_commit(barM);
+        }
+        done = tc_wait(barM, 1, 1L << 26);
+        if (!done) pending = 1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        ok = __syncthreads_and(done ? 1 : 0) != 0;
+    }
+    ok = ok && !*bfail;
+    double* cq = static_cast<double*>(d.cq);
     if (ok) {
         const uint32_t trow = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
@@ -870,14 +902,24 @@ __device__ void mm_z_tc(const MmDesc& d, int tile, unsigned char* smem) {
 #pragma unroll
             for (int e = 0; e < 16; e++)
                 if (c + e < r) zq[(size_t)(c + e) * N + t] = v[e];
+            if (adj) {
+                tc_ld16(trow + (uint32_t)(32 + c), v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int e = 0; e < 16; e++)
+                    if (c + e < r) cq[(size_t)(c + e) * N + t] = (double)v[e];
+            }
         }
     } else {
 #pragma unroll 1
-        for (int k = 0; k < r; k++) zq[(size_t)k * N + t] = __int_as_float(0x7fc00000);
+        for (int k = 0; k < r; k++) {
+            zq[(size_t)k * N + t] = __int_as_float(0x7fc00000);
+            if (adj) cq[(size_t)k * N + t] = __longlong_as_double(0x7ff8000000000000LL);
+        }
     }
     if (tid == 0) {
         if (*bfail) tc_wait(barB, 0, 1L << 26);
-        if (!done) tc_wait(barM, 0, 1L << 30);
+        if (pending >= 0) tc_wait(barM, (uint32_t)pending, 1L << 30);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
