@@ -190,20 +190,40 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
             if (st.stage < 6) {
                 // a checkpoint due at this step's start (set by the control kernel)
                 const int ckp = ph == PH_FWD && st.stage == 1 ? st.ck_pend : 0;
+                // stage-outer, point-inner over chunks of SC points: each
+                // stage's loads of a chunk are in flight together (the
+                // per-point sum still runs over the stages in order)
+                constexpr int SC = E < 8 ? E : 8;
 #pragma unroll
-                for (int s = 0; s < E; s++) {
-                    const size_t b = off + tid + TT * s;
-                    double ar = 0.0, ai = 0.0;
+                for (int s0 = 0; s0 < E; s0 += SC) {
+                    double ar[SC], ai[SC];
+#pragma unroll
+                    for (int c = 0; c < SC; c++) ar[c] = ai[c] = 0.0;
+#pragma unroll 1
                     for (int j = 0; j < st.stage; j++) {
-                        const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
+                        const C* __restrict__ kj = static_cast<const C*>(mm_kp(K, perm, j));
                         const double a = kT5a[st.stage][j];
-                        ar += a * (double)kj.re;
-                        ai += a * (double)kj.im;
-                        if (ckp && j == 0) static_cast<C*>(d.ck_k1)[(size_t)(ckp - 1) * NM + b] = kj;
+                        C xk[SC];
+#pragma unroll
+                        for (int c = 0; c < SC; c++) xk[c] = kj[off + tid + TT * (s0 + c)];
+#pragma unroll
+                        for (int c = 0; c < SC; c++) {
+                            ar[c] += a * (double)xk[c].re;
+                            ai[c] += a * (double)xk[c].im;
+                        }
+                        if (ckp && j == 0) {
+#pragma unroll
+                            for (int c = 0; c < SC; c++)
+                                static_cast<C*>(d.ck_k1)[(size_t)(ckp - 1) * NM + off + tid + TT * (s0 + c)] = xk[c];
+                        }
                     }
-                    const cx<double> un = ld2(x, b);
-                    if (ckp) st2(d.ck_u, (size_t)(ckp - 1) * NM + b, un);
-                    v[s] = mk((R)(un.re + dt * ar), (R)(un.im + dt * ai));
+#pragma unroll
+                    for (int c = 0; c < SC; c++) {
+                        const size_t b = off + tid + TT * (s0 + c);
+                        const cx<double> un = ld2(x, b);
+                        if (ckp) st2(d.ck_u, (size_t)(ckp - 1) * NM + b, un);
+                        v[s0 + c] = mk((R)(un.re + dt * ar[c]), (R)(un.im + dt * ai[c]));
+                    }
                 }
             } else {
                 double* xnew = fw ? d.u[cur ^ 1] : d.lam[cur ^ 1];
