@@ -53,7 +53,12 @@ extern "C" {
                                 index left its buffer's bounds; the slot stopped before
                                 the access */
 
-#define FL_PRECISION_FP32 0  /* FP32 bulk, FP64 phase/norm/reductions/state */
+/* FP32 bulk, FP64 phase/norm/reductions/state.  The single-mode adjoint runs
+ * in FP64; the multimode adjoint (M >= 6, Nt a multiple of 128) keeps λ and
+ * its transforms in FP64 and takes the forward field's transform, pair
+ * products and the per-point contractions at FP32 accuracy (3xTF32 tensor
+ * cores, low-rank form of the overlap contraction where γ allows it). */
+#define FL_PRECISION_FP32 0
 #define FL_PRECISION_FP64 1  /* all arithmetic in FP64 */
 
 typedef struct fl_ctx fl_ctx;
