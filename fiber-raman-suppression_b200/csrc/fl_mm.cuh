@@ -229,28 +229,43 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
                 double* xnew = fw ? d.u[cur ^ 1] : d.lam[cur ^ 1];
                 const bool want_err = ph != PH_REC;
                 const double at = fw ? d.abstol : st.abstol_adj, rt = d.reltol;
+                // chunks of SC6 points, the six stages' loads of a chunk in
+                // flight together (two sums per point: solution and error)
+                constexpr int SC6 = E < 4 ? E : 4;
 #pragma unroll
-                for (int s = 0; s < E; s++) {
-                    const size_t b = off + tid + TT * s;
-                    double ar = 0.0, ai = 0.0, er = 0.0, ei = 0.0;
+                for (int s0 = 0; s0 < E; s0 += SC6) {
+                    double ar[SC6], ai[SC6], er[SC6], ei[SC6];
+#pragma unroll
+                    for (int c = 0; c < SC6; c++) ar[c] = ai[c] = er[c] = ei[c] = 0.0;
+#pragma unroll
                     for (int j = 0; j < 6; j++) {
-                        const C kj = static_cast<const C*>(mm_kp(K, perm, j))[b];
+                        const C* __restrict__ kj = static_cast<const C*>(mm_kp(K, perm, j));
                         const double a = kT5a[6][j], bt = kT5bt[j];
-                        ar += a * (double)kj.re;
-                        ai += a * (double)kj.im;
-                        er += bt * (double)kj.re;
-                        ei += bt * (double)kj.im;
+                        C xk[SC6];
+#pragma unroll
+                        for (int c = 0; c < SC6; c++) xk[c] = kj[off + tid + TT * (s0 + c)];
+#pragma unroll
+                        for (int c = 0; c < SC6; c++) {
+                            ar[c] += a * (double)xk[c].re;
+                            ai[c] += a * (double)xk[c].im;
+                            er[c] += bt * (double)xk[c].re;
+                            ei[c] += bt * (double)xk[c].im;
+                        }
                     }
-                    const cx<double> un = ld2(x, b);
-                    const cx<double> u1 = mk(un.re + dt * ar, un.im + dt * ai);
-                    st2(xnew, b, u1);
-                    if (want_err) {
-                        st2(d.esv, b, mk(dt * er, dt * ei));
-                        const double m0 = sqrt(un.re * un.re + un.im * un.im);
-                        const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
-                        d.skv[b] = at + fmax(m0, m1) * rt;
+#pragma unroll
+                    for (int c = 0; c < SC6; c++) {
+                        const size_t b = off + tid + TT * (s0 + c);
+                        const cx<double> un = ld2(x, b);
+                        const cx<double> u1 = mk(un.re + dt * ar[c], un.im + dt * ai[c]);
+                        st2(xnew, b, u1);
+                        if (want_err) {
+                            st2(d.esv, b, mk(dt * er[c], dt * ei[c]));
+                            const double m0 = sqrt(un.re * un.re + un.im * un.im);
+                            const double m1 = sqrt(u1.re * u1.re + u1.im * u1.im);
+                            d.skv[b] = at + fmax(m0, m1) * rt;
+                        }
+                        v[s0 + c] = down<R>(u1);
                     }
-                    v[s] = down<R>(u1);
                 }
             }
         }
@@ -474,22 +489,37 @@ __global__ void __launch_bounds__(MmGroup<R, LOGN, LOGE, CL>::T, 1)
                      base = (size_t)(keep_rec ? sb.seg_lo + st.rec_pos - sb.lo : st.nsteps) * 5 * NM;
         C* sg = static_cast<C*>(d.seg);
         const double* un = d.u[st.cur];
-#pragma unroll 1
-        for (int s = 0; s < E; s++) {
-            const size_t b = off + tid + TT * s;
-            sg[base + b] = down<R>(ld2(un, b));
-            double cr[4] = {0, 0, 0, 0}, ci[4] = {0, 0, 0, 0};
+        // pairs of points, the six stored stages' loads of a pair in flight
+        // together (the per-point sums run over the stages in order)
+#pragma unroll
+        for (int s0 = 0; s0 < E; s0 += 2) {
+            double cr[2][4], ci[2][4];
+#pragma unroll
+            for (int c = 0; c < 2; c++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) cr[c][q] = ci[c][q] = 0.0;
 #pragma unroll
             for (int i = 0; i < 7; i++) {
-                const C ki = i == 6 ? v[s] : static_cast<const C*>(mm_kp(d.kf, st.kperm, i))[b];
+                C ki[2];
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    cr[q] += kT5r[i][q] * (double)ki.re;
-                    ci[q] += kT5r[i][q] * (double)ki.im;
-                }
+                for (int c = 0; c < 2; c++)
+                    ki[c] = i == 6 ? v[s0 + c]
+                                   : static_cast<const C*>(mm_kp(d.kf, st.kperm, i))[off + tid + TT * (s0 + c)];
+#pragma unroll
+                for (int c = 0; c < 2; c++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        cr[c][q] += kT5r[i][q] * (double)ki[c].re;
+                        ci[c][q] += kT5r[i][q] * (double)ki[c].im;
+                    }
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++) sg[base + (q + 1) * NM + b] = mk((R)cr[q], (R)ci[q]);
+            for (int c = 0; c < 2; c++) {
+                const size_t b = off + tid + TT * (s0 + c);
+                sg[base + b] = down<R>(ld2(un, b));
+#pragma unroll
+                for (int q = 0; q < 4; q++) sg[base + (q + 1) * NM + b] = mk((R)cr[c][q], (R)ci[c][q]);
+            }
         }
     }
     if (st.stage == 6 && (ph == PH_FWD || ph == PH_ADJ)) {
