@@ -525,9 +525,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     w->per_mode = per_mode;
     const size_t nm = (size_t)pr->nt * pr->m, npn = (size_t)w->np * pr->nt;
     const int nparts = pr->m * mm_cluster_ctas(ilog2i(pr->nt));
-    const int nparts64 = pr->m * mm_cluster_ctas64(ilog2i(pr->nt));
-    const int npart_max = std::max(nparts, nparts64);
-    const size_t per = mm_slot_bytes(nm, npn, rf, w->K, w->segcap, w->stepcap, npart_max);
+    const size_t per = mm_slot_bytes(nm, npn, rf, w->K, w->segcap, w->stepcap, nparts);
     const size_t io = 16 * nm * (4 + nsave) + 8 * nm + 256 * 8;
     w->pool_bytes = (per + io) * (size_t)B + 16 * (size_t)std::max(nsave, 1) + pr->nt + 4096;
     if (o.hbm_budget_bytes && w->pool_bytes > o.hbm_budget_bytes)
@@ -568,7 +566,6 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         d.Utcs = pr->d_Utcs;
         d.M = pr->m;
         d.nparts = nparts;
-        d.nparts64 = nparts64;
         d.NP = w->np;
         d.N = pr->nt;
         d.fp64 = pr->precision == FL_PRECISION_FP64;
@@ -600,7 +597,7 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
         d.probe = carve(p, D2);
         d.esv = (double*)carve(p, D2);
         d.skv = (double*)carve(p, 8 * nm);
-        d.part = (double*)carve(p, 8 * (size_t)npart_max);
+        d.part = (double*)carve(p, 8 * (size_t)nparts);
         d.ck_u = (double*)carve(p, D2 * w->K);
         d.ck_k1 = carve(p, C * w->K);
         d.steplog = (double*)carve(p, 16 * (size_t)w->stepcap);
@@ -1211,14 +1208,14 @@ size_t srv_slot_bytes(const fl_server* sv, const fl_problem* pr) {
                             16 * (size_t)pr->nt * 4 + 8 * (size_t)pr->nt + 2 * (size_t)pr->nt;
     const size_t nm = (size_t)pr->nt * pr->m, np = (size_t)pr->m * (pr->m + 1) / 2;
     return mm_slot_bytes(nm, np * pr->nt, rf, o.checkpoints, o.segment_steps, step_log_entries(o),
-                         pr->m * std::max(mm_cluster_ctas(ilog2i(pr->nt)), mm_cluster_ctas64(ilog2i(pr->nt)))) +
+                         pr->m * mm_cluster_ctas(ilog2i(pr->nt))) +
            16 * nm * 4 + 8 * nm + 2 * (size_t)pr->nt;
 }
 
 int srv_chunk_slots(const fl_server* sv, const SrvBucket* b) {
     const int cap = std::max(1, std::min(sv->opts.max_active_ctas, std::max(1, sv->ctx->sm_count)));
     if (!b->mm) return cap;
-    return std::max(1, cap / (b->m * std::max(mm_cluster_ctas(ilog2i(b->nt)), mm_cluster_ctas64(ilog2i(b->nt)))));
+    return std::max(1, cap / (b->m * mm_cluster_ctas(ilog2i(b->nt))));
 }
 
 // a bucket's own table set: a problem with this shape's grid (zero tables),
@@ -2434,7 +2431,7 @@ int fl_server_submit(fl_server* sv, const fl_request* q, long* id) {
     if (!std::isfinite(L)) return set_err(ctx, FL_EINVAL, "L must be positive and finite");
     auto r = std::make_unique<SrvRequest>();
     r->prob = pr;
-    r->weight = pr->use_mm ? pr->m * std::max(mm_cluster_ctas(logn), mm_cluster_ctas64(logn)) : 1;
+    r->weight = pr->use_mm ? pr->m * mm_cluster_ctas(logn) : 1;
     r->kind = q->kind;
     r->log_cost = q->log_cost;
     r->objective = pr->objective;

@@ -880,8 +880,7 @@ struct MmCtl {
                 return;
             }
             double acc = 0.0;
-            const int np = d.fp64 ? d.nparts64 : d.nparts;  // the epilogue's transform shape
-            for (int m = 0; m < np; m++) acc += d.part[m];
+            for (int m = 0; m < d.nparts; m++) acc += d.part[m];
             const double EEst = sqrt(acc / (double)NM);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;
@@ -989,7 +988,7 @@ struct MmCtl {
             const double z = st.cz, dt = st.cdt;
             const double zlo = d.steplog[2 * sub_segment(d, st).lo];
             double acc = 0.0;
-            for (int m = 0; m < d.nparts64; m++) acc += d.part[m];  // (FP64 epilogue)
+            for (int m = 0; m < d.nparts; m++) acc += d.part[m];
             const double EEst = sqrt(acc / (double)NM);
             if (!isfinite(EEst)) {
                 st.status = ST_NONFINITE;

@@ -37,7 +37,6 @@ EvidenceFn mm_evidence_launcher(int logn) {
 }
 
 int mm_cluster_ctas(int logn) { return logn == 15 ? 4 : 1; }
-int mm_cluster_ctas64(int logn) { return logn == 15 ? 4 : logn == 14 ? 2 : 1; }
 
 bool mm_supported_modes(int M) { return M >= 2 && M <= 10; }
 

@@ -42,11 +42,9 @@ cudaError_t mm_launch_fft_kernels(const MmRound& a, int which) {
     }
 }
 
-// one evaluation round; the FP64 transforms may take their own shape (LOGE64
-// values per thread over CL64 CTAs: at Nt = 2^14 an FP64 field does not fit
-// one CTA's registers); each stage's launches sit in a named NVTX range
+// one evaluation round; each stage's launches sit in a named NVTX range
 // (host-side: under graph capture the ranges mark the capture)
-template <int LOGN, int LOGE, int CL, int LOGE64, int CL64>
+template <int LOGN, int LOGE, int CL>
 cudaError_t mm_round(const MmRound& a) {
     cudaError_t e;
 #define FL_TRY(x)                        \
@@ -56,7 +54,7 @@ cudaError_t mm_round(const MmRound& a) {
     }
     nvtxRangePushA("fl: mm prologue");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 0)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE64, CL64>(a, 0)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 0)));
     nvtxRangePop();
     nvtxRangePushA("fl: mm Im X contraction");
     FL_TRY(mm_launch_contract(a, 1));
@@ -66,7 +64,7 @@ cudaError_t mm_round(const MmRound& a) {
     nvtxRangePop();
     nvtxRangePushA("fl: mm pairs");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 1)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE64, CL64>(a, 1)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 1)));
     nvtxRangePop();
     nvtxRangePushA("fl: mm contraction");
     FL_TRY(mm_launch_contract(a, 0));
@@ -74,7 +72,7 @@ cudaError_t mm_round(const MmRound& a) {
     nvtxRangePop();
     nvtxRangePushA("fl: mm epilogue");
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 2)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE64, CL64>(a, 2)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 2)));
     nvtxRangePop();
     if (a.control) {
         nvtxRangePushA("fl: mm control");
@@ -87,13 +85,10 @@ cudaError_t mm_round(const MmRound& a) {
 
 }  // namespace fl
 
-#define FL_MM_INSTANCE2(LOGN, LOGE, CL, LOGE64, CL64)                                        \
-    namespace fl {                                                                            \
-    cudaError_t mm_round_##LOGN(const MmRound& a) {                                           \
-        return mm_round<LOGN, LOGE, CL, LOGE64, CL64>(a);                                     \
-    }                                                                                         \
-    cudaError_t mm_evidence_##LOGN(const EvidenceArgs& a) {                                   \
-        return launch_evidence<LOGN, LOGE64, CL64>(a);                                        \
-    }                                                                                         \
+#define FL_MM_INSTANCE(LOGN, LOGE, CL)                                                     \
+    namespace fl {                                                                         \
+    cudaError_t mm_round_##LOGN(const MmRound& a) { return mm_round<LOGN, LOGE, CL>(a); } \
+    cudaError_t mm_evidence_##LOGN(const EvidenceArgs& a) {                                \
+        return launch_evidence<LOGN, LOGE, CL>(a);                                         \
+    }                                                                                      \
     }
-#define FL_MM_INSTANCE(LOGN, LOGE, CL) FL_MM_INSTANCE2(LOGN, LOGE, CL, LOGE, CL)

@@ -47,7 +47,6 @@ cudaError_t mm_launch_contract(const MmRound& a, int which);  // 0 fwd, 1 Im X, 
 cudaError_t mm_launch_control(const MmRound& a, int consume);
 bool mm_supported_modes(int M);
 // CTAs (one cluster) per transform at Nt = 2^logn
-int mm_cluster_ctas(int logn);    // CTAs per FP32 transform
-int mm_cluster_ctas64(int logn);  // CTAs per FP64 transform
+int mm_cluster_ctas(int logn);
 
 }  // namespace fl

@@ -148,8 +148,7 @@ struct MmDesc {
     const float* Utcs;      // B of the adjoint's D': rows p = (i <= j), K = k
     int M, NP, N, fp64;     // modes, pairs M(M+1)/2, points, forward precision
     int adj_mixed;          // mm_adj_mixed(M, N, fp64): mixed-precision adjoint
-    int nparts;             // error partial sums per FP32 evaluation (M x CTAs per transform)
-    int nparts64;           // and per FP64 evaluation
+    int nparts;             // error partial sums per evaluation (M x CTAs per transform)
     double one_m_fR;
     double L, reltol, abstol;
     int mode, log_cost, nsave;
