@@ -331,8 +331,7 @@ int work_create(fl_problem* pr, int B, int nsave, int mode, Work** out,
     return FL_OK;
 }
 
-int launch_slots(fl_ctx* ctx, fl_problem* pr, Work* w, int nactive, int max_evals,
-                 int split_forward = 0) {
+int launch_slots(fl_ctx* ctx, fl_problem* pr, Work* w, int nactive, int max_evals) {
     const int logn = ilog2i(pr->nt);
     const int fp64 = pr->precision == FL_PRECISION_FP64;
     LaunchFn fn = sm_launcher(fp64, logn);
@@ -340,9 +339,8 @@ int launch_slots(fl_ctx* ctx, fl_problem* pr, Work* w, int nactive, int max_eval
         return set_err(ctx, FL_EUNSUPPORTED, "Nt = 2^%d is not built for %s", logn,
                        fp64 ? "FP64" : "FP32");
     LaunchArgs a{w->d_desc, w->d_state, w->d_active, nactive, max_evals, ctx->stream};
-    a.split_forward = split_forward && !fp64 && logn == 13;
     CU(fn(a));
-    ctx->launches += a.split_forward ? 2 : 1;
+    ctx->launches++;
     return FL_OK;
 }
 
@@ -350,7 +348,7 @@ int run_to_completion(fl_problem* pr, Work* w) {
     Nvtx nvtx_("fl: single-mode stepper (run to completion)");
     fl_ctx* ctx = pr->ctx;
     CU(cudaEventRecord(ctx->ev[2], ctx->stream));
-    int rc = launch_slots(ctx, pr, w, w->B, 0x7fffffff, 1);
+    int rc = launch_slots(ctx, pr, w, w->B, 0x7fffffff);
     if (rc) return rc;
     CU(cudaEventRecord(ctx->ev[3], ctx->stream));
     CU(cudaStreamSynchronize(ctx->stream));

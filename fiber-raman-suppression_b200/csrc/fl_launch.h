@@ -14,9 +14,6 @@ struct LaunchArgs {
     int nactive;
     int max_evals;         // RHS evaluations per slot in this launch
     cudaStream_t stream;
-    // run to completion: at Nt = 2^13 (FP32 forward, FP64 adjoint) take every
-    // slot to its seed with the forward-only kernel (two CTAs per SM) first
-    int split_forward = 0;
 };
 
 using LaunchFn = cudaError_t (*)(const LaunchArgs&);

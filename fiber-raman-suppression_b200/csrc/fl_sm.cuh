@@ -957,13 +957,11 @@ __device__ __forceinline__ double init_after_f1(const double* x0, const cx<K>* k
 
 // The state machine.  Each loop iteration performs at most one RHS
 // evaluation (forward in RF, adjoint in RA) plus the bookkeeping around it,
-// so the FFT code exists once per precision in the kernel.  FWD: the
-// forward-only form, which stops at the seed (PH_SEED) and uses no tensor
-// memory (its RHS scratch is the slot's global scr fields).
-template <typename RF, typename RA, int LOGN, int LOGE, bool FWD>
-__device__ __forceinline__ void sm_advance_body(const SlotDesc* __restrict__ descs,
-                                                SlotState* __restrict__ states,
-                                                const int* __restrict__ active, int max_evals) {
+// so the FFT code exists once per precision in the kernel.
+template <typename RF, typename RA, int LOGN, int LOGE>
+__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
+    sm_advance_kernel(const SlotDesc* __restrict__ descs, SlotState* __restrict__ states,
+                      const int* __restrict__ active, int max_evals) {
     using SolF = SmSolver<RF, LOGN, LOGE>;
     using SolA = SmSolver<RA, LOGN, LOGE>;
     using CF = cx<RF>;
@@ -974,7 +972,7 @@ __device__ __forceinline__ void sm_advance_body(const SlotDesc* __restrict__ des
 
     const int slot = active[blockIdx.x];
     const SlotDesc& d = descs[slot];
-    const uint32_t tm = FWD ? kNoTmem : tm_alloc<LOGN, LOGE>(tm_slot<RA, LOGN>(smraw));
+    const uint32_t tm = tm_alloc<LOGN, LOGE>(tm_slot<RA, LOGN>(smraw));
     load_twiddles<LOGN>(d, red);
     SlotState st = states[slot];  // block-uniform copy
     SolF SF(d, smraw, red);
@@ -989,7 +987,7 @@ __device__ __forceinline__ void sm_advance_body(const SlotDesc* __restrict__ des
     const IOA va{IOA::SMEM ? reinterpret_cast<CA*>(smraw) : val};
     int evals = 0;
 
-    while (st.phase != PH_DONE && !(FWD && st.phase == PH_SEED) && evals < max_evals) {
+    while (st.phase != PH_DONE && evals < max_evals) {
 #ifdef FL_CHECKED
         if (!state_in_bounds(d, st)) {
             st.status = ST_CHECK;
@@ -1492,26 +1490,7 @@ __device__ __forceinline__ void sm_advance_body(const SlotDesc* __restrict__ des
     }
     __syncthreads();
     if (tid == 0) states[slot] = st;
-    if (!FWD) tm_free<LOGN, LOGE>(tm);
-}
-
-template <typename RF, typename RA, int LOGN, int LOGE>
-__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 1)
-    sm_advance_kernel(const SlotDesc* __restrict__ descs, SlotState* __restrict__ states,
-                      const int* __restrict__ active, int max_evals) {
-    sm_advance_body<RF, RA, LOGN, LOGE, false>(descs, states, active, max_evals);
-}
-
-// The forward-only form at two CTAs per SM: the forward phases (FP32
-// transforms, no tensor-memory scratch) take a quarter of the shared memory
-// and half the registers of the FP64 adjoint's, so a run-to-completion batch
-// first takes every slot to its seed with this kernel, then continues with
-// sm_advance_kernel.
-template <typename RF, int LOGN, int LOGE>
-__global__ void __launch_bounds__(FftShape<LOGN, LOGE>::T, 2)
-    sm_forward_kernel(const SlotDesc* __restrict__ descs, SlotState* __restrict__ states,
-                      const int* __restrict__ active, int max_evals) {
-    sm_advance_body<RF, RF, LOGN, LOGE, true>(descs, states, active, max_evals);
+    tm_free<LOGN, LOGE>(tm);
 }
 
 }  // namespace fl

@@ -8,21 +8,6 @@ namespace fl {
 template <typename RF, typename RA, int LOGN, int LOGE>
 cudaError_t launch_sm(const LaunchArgs& a) {
     using S = FftShape<LOGN, LOGE>;
-    if constexpr (sizeof(RF) == 4 && sizeof(RA) == 8 && LOGN == 13) {
-        if (a.split_forward) {
-            // 256 threads of 32 values: two CTAs per SM at 128 registers
-            // (the global fields are indexed by bin, whatever the CTA shape)
-            constexpr int LOGEF = 5;
-            auto fk = sm_forward_kernel<RF, LOGN, LOGEF>;
-            const size_t fs = smem_bytes<RF, LOGN>();
-            cudaError_t e = cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)fs);
-            if (e != cudaSuccess) return e;
-            fk<<<a.nactive, FftShape<LOGN, LOGEF>::T, fs, a.stream>>>(
-                static_cast<const SlotDesc*>(a.desc), a.state, a.active, a.max_evals);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        }
-    }
     auto kern = sm_advance_kernel<RF, RA, LOGN, LOGE>;
     const size_t smem = smem_bytes<RA, LOGN>();
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
