@@ -646,6 +646,8 @@ MmRound mm_round_args(fl_problem* pr, MmWork* w, int nactive) {
     a.NP = w->np;
     a.N = pr->nt;
     a.fp64 = pr->precision == FL_PRECISION_FP64;
+    a.lowrank_some = pr->rank > 0;  // one problem per batch
+    a.fullrank_some = pr->rank == 0;
     a.control = 1;
     a.tensor_cores = 1;
     a.ndone = nullptr;

@@ -187,7 +187,7 @@ cudaError_t contract_m(const MmRound& a, int which) {
     // slots without a low-rank form skip it)
     if (which == 3) {
         if constexpr (M >= 6) {
-            if (mm_adj_mixed(M, a.N, a.fp64)) return z_tc<M>(a);
+            if (mm_adj_mixed(M, a.N, a.fp64) && a.lowrank_some) return z_tc<M>(a);
         }
         return cudaSuccess;
     }
@@ -199,7 +199,8 @@ cudaError_t contract_m(const MmRound& a, int which) {
     // contractions and the Im X contraction on the tensor cores (3xTF32)
     if constexpr (sizeof(R) == 8 && M >= 6) {
         if (which == 2 && mm_adj_mixed(M, a.N, a.fp64)) return contract_adj_tc<M>(a);
-        if (which == 1 && mm_adj_mixed(M, a.N, a.fp64)) return imx_tc<M>(a);
+        if (which == 1 && mm_adj_mixed(M, a.N, a.fp64))
+            return a.fullrank_some ? imx_tc<M>(a) : cudaSuccess;
     }
     const int n = which == 2 ? a.N * M : a.N;
     const dim3 grid((n + kMmTB - 1) / kMmTB, a.nactive);

@@ -17,6 +17,10 @@ struct MmRound {
     int fp64;              // forward precision of the batch
     int control;           // run the control kernel after the evaluation
     int tensor_cores;      // FP32 forward contraction on tcgen05 when M >= 6
+    // slots with and without a low-rank form (rank > 0) may be in the batch:
+    // the Z kernel serves the first, the Im X kernel the second; a kind known
+    // to be absent is not launched
+    int lowrank_some = 1, fullrank_some = 1;
     int* ndone;            // control: count of finished slots (nullable)
     cudaStream_t stream;
 };
