@@ -1,5 +1,9 @@
-// fl_tc.cuh -- forward Kerr/Raman contraction of the multimode stepper on the
-// 5th-generation tensor cores (tcgen05, sm_100a), for M >= 6 modes.
+// fl_tc.cuh -- the multimode stepper's per-time-point contractions on the
+// 5th-generation tensor cores (tcgen05, sm_100a), for M >= 6 modes: the
+// forward Kerr/Raman contraction (below), the adjoint's Im X reduction and
+// assembly (mm_imx_tc, mm_contract_adj_tc) and the low-rank form's
+// reductions (mm_z_tc).  In the low-rank form (rank > 0) the forward GEMM
+// takes B = U and A = S̃ (K = the rank padded to 8) instead of G and S.
 //
 // Per time point t the forward contraction is δ_ij(t) = Σ_q G[ij][q] S_q(t)
 // followed by η_i = Σ_j δ_ij u_j (simulate_disp_mmf.jl:38-53 with the Raman
@@ -21,7 +25,8 @@
 // thread waits on it with a bounded spin (on timeout the tile's outputs are
 // set to NaN, which the error norm turns into FL_NONFINITE) and then reads
 // its own row of D with tcgen05.ld.  Tensor memory is allocated per CTA
-// (128 columns) and freed before the CTA exits on every path.
+// (128 columns for the forward GEMM) and freed before the CTA exits on every
+// path.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
