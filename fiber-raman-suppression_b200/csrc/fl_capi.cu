@@ -479,9 +479,15 @@ struct MmWork {
     // mm_run's batch of evaluation rounds as a CUDA graph, for graph_nactive slots
     cudaGraphExec_t graph = nullptr;
     int graph_nactive = -1;
+    // the rounds' side stream and its fork / join events
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
     ~MmWork() {
         if (graph) cudaGraphExecDestroy(graph);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         cudaFree(pool);
         cudaFree(d_desc);
         cudaFree(d_state);
@@ -534,6 +540,9 @@ int mm_work_create(fl_problem* pr, int B, int nsave, int mode, int per_mode, MmW
     CU(cudaMalloc(&w->pool, w->pool_bytes));
     CU(cudaMalloc(&w->d_desc, sizeof(MmDesc) * B));
     CU(cudaMalloc(&w->d_state, sizeof(MmState) * B));
+    CU(cudaStreamCreateWithFlags(&w->side, cudaStreamNonBlocking));
+    CU(cudaEventCreateWithFlags(&w->ev_fork, cudaEventDisableTiming));
+    CU(cudaEventCreateWithFlags(&w->ev_join, cudaEventDisableTiming));
     CU(cudaMalloc(&w->d_active, sizeof(int) * B));
     CU(cudaMalloc(&w->d_ndone, sizeof(int)));
     CU(cudaMallocHost(&w->h_ndone, sizeof(int)));
@@ -648,6 +657,9 @@ MmRound mm_round_args(fl_problem* pr, MmWork* w, int nactive) {
     a.fp64 = pr->precision == FL_PRECISION_FP64;
     a.lowrank_some = pr->rank > 0;  // one problem per batch
     a.fullrank_some = pr->rank == 0;
+    a.side = w->side;
+    a.ev_fork = w->ev_fork;
+    a.ev_join = w->ev_join;
     a.control = 1;
     a.tensor_cores = 1;
     a.ndone = nullptr;

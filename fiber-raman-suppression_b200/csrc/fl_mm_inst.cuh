@@ -52,9 +52,27 @@ cudaError_t mm_round(const MmRound& a) {
         nvtxRangePop();                  \
         return e;                        \
     }
+    // FP32 batches with a side stream: each stage's FP64 kernel runs on it,
+    // beside the FP32 one (the two serve forward and adjoint slots, or write
+    // the forward field's and λ's buffers), joined before the next stage
+    const bool two = a.side != nullptr && !a.fp64;
+    MmRound b = a;
+    if (two) b.stream = a.side;
+    auto fork = [&]() -> cudaError_t {
+        if (!two) return cudaSuccess;
+        cudaError_t x = cudaEventRecord(a.ev_fork, a.stream);
+        return x == cudaSuccess ? cudaStreamWaitEvent(a.side, a.ev_fork, 0) : x;
+    };
+    auto join = [&]() -> cudaError_t {
+        if (!two) return cudaSuccess;
+        cudaError_t x = cudaEventRecord(a.ev_join, a.side);
+        return x == cudaSuccess ? cudaStreamWaitEvent(a.stream, a.ev_join, 0) : x;
+    };
     nvtxRangePushA("fl: mm prologue");
+    FL_TRY(fork());
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 0)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 0)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(b, 0)));
+    FL_TRY(join());
     nvtxRangePop();
     nvtxRangePushA("fl: mm Im X contraction");
     FL_TRY(mm_launch_contract(a, 1));
@@ -63,16 +81,22 @@ cudaError_t mm_round(const MmRound& a) {
     FL_TRY(mm_launch_contract(a, 3));
     nvtxRangePop();
     nvtxRangePushA("fl: mm pairs");
+    FL_TRY(fork());
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 1)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 1)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(b, 1)));
+    FL_TRY(join());
     nvtxRangePop();
     nvtxRangePushA("fl: mm contraction");
+    FL_TRY(fork());
     FL_TRY(mm_launch_contract(a, 0));
-    FL_TRY(mm_launch_contract(a, 2));
+    FL_TRY(mm_launch_contract(b, 2));
+    FL_TRY(join());
     nvtxRangePop();
     nvtxRangePushA("fl: mm epilogue");
+    FL_TRY(fork());
     if (!a.fp64) FL_TRY((mm_launch_fft_kernels<float, LOGN, LOGE, CL>(a, 2)));
-    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(a, 2)));
+    FL_TRY((mm_launch_fft_kernels<double, LOGN, LOGE, CL>(b, 2)));
+    FL_TRY(join());
     nvtxRangePop();
     if (a.control) {
         nvtxRangePushA("fl: mm control");

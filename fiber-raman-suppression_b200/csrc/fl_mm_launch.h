@@ -21,6 +21,11 @@ struct MmRound {
     // the Z kernel serves the first, the Im X kernel the second; a kind known
     // to be absent is not launched
     int lowrank_some = 1, fullrank_some = 1;
+    // a side stream (with two events) on which a stage's FP64 kernels run
+    // beside its FP32 ones: they serve different slots or write different
+    // buffers (nullptr: one stream)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int* ndone;            // control: count of finished slots (nullable)
     cudaStream_t stream;
 };
